@@ -1,0 +1,835 @@
+// C ABI of the grid-map engine: contexts, device buffers, the e-map and
+// affinity entry points, whole-job (GPF) entry points and the command line.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <signal.h>
+#include <string>
+#include <sys/wait.h>
+#include <unistd.h>
+#include <vector>
+
+#include "../../include/fastgrid_b200.h"
+#include "ag_host.h"
+#include "ag_kernels.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess) return fail(AG_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Threshold table for the exact e-map bin: thr[k] is the least double r^2
+// with int(sqrt(r^2) * 100.0) >= k under IEEE double rounding, i.e. the bin
+// the reference's FP64 code (Cpu.cpp:70-75) computes is k-1 below it and k
+// at or above it.
+const std::vector<double>& binThresholds() {
+  static std::vector<double> thr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    thr.assign(agk::kNX > 0 ? 8193 : 0, 0.0);
+    auto binOf = [](double r2) { return sqrt(r2) * 100.0; };
+    for (int k = 1; k <= 8192; k++) {
+      double lo = 0.0, hi = (k / 100.0 + 1.0) * (k / 100.0 + 1.0);
+      uint64_t a, b;
+      memcpy(&a, &lo, 8);
+      memcpy(&b, &hi, 8);
+      while (b - a > 1) {
+        uint64_t m = a + (b - a) / 2;
+        double v;
+        memcpy(&v, &m, 8);
+        if (binOf(v) >= (double)k) b = m; else a = m;
+      }
+      memcpy(&thr[k], &b, 8);
+    }
+  });
+  return thr;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct ag_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  // e-map
+  DevBuf<double4> atoms;
+  DevBuf<float> epsTab;
+  DevBuf<double> thr;
+  DevBuf<int> items;
+  DevBuf<agk::EmapBlock> blocks;
+  DevBuf<double> partial;
+  DevBuf<float> maps;
+  DevBuf<unsigned> status;
+  std::vector<int> hItems;
+  std::vector<agk::EmapBlock> hBlocks;
+  int itemsFor[3] = {0, 0, 0};
+  double itemsH = 0;
+  // affinity
+  DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
+  DevBuf<float> vol, solq, affTab, affTabH, sol;
+  DevBuf<double> rv, rv2;
+  // job
+  bool haveJob = false, haveAff = false, ddd = true;
+  ag_grid grid{};
+  int nAtoms = 0, nMaps = 0, nTypes = 0, hydrogen = -1;
+  double solparQ = 0;
+  std::vector<int> mapHbond, mapIsHB, mapCov;
+  std::vector<float> solparProbe, volProbe;
+  int emapMode = agk::kEmapKahan;
+  float rNear = 14.0f;
+  float delta = 2.0e-3f;
+  int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
+};
+
+extern "C" const char* ag_last_error(void) { return g_err.c_str(); }
+
+extern "C" int ag_ctx_create(int device, ag_ctx** out) {
+  if (!out) return fail(AG_E_INVALID, "null output pointer");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(AG_E_CUDA, "no CUDA device is available; this engine has no CPU fallback");
+  if (device < 0 || device >= n) return fail(AG_E_INVALID, "device %d out of range (%d devices)", device, n);
+  CK(cudaSetDevice(device));
+  auto* c = new ag_ctx();
+  c->device = device;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return fail(AG_E_CUDA, "cudaStreamCreate failed");
+  }
+  if (c->status.ensure(4) != cudaSuccess) {
+    delete c;
+    return fail(AG_E_NOMEM, "cannot allocate the status word");
+  }
+  const auto& thr = binThresholds();
+  if (c->thr.ensure(thr.size()) != cudaSuccess ||
+      cudaMemcpy(c->thr.p, thr.data(), thr.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    delete c;
+    return fail(AG_E_CUDA, "cannot upload the bin threshold table");
+  }
+  *out = c;
+  return AG_OK;
+}
+
+extern "C" int ag_ctx_destroy(ag_ctx* c) {
+  if (!c) return AG_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto* b : {&c->epsTab, &c->maps, &c->vol, &c->solq, &c->affTab, &c->affTabH, &c->sol}) b->release();
+  c->atoms.release();
+  c->thr.release();
+  c->partial.release();
+  c->rv.release();
+  c->rv2.release();
+  c->blocks.release();
+  c->status.release();
+  for (auto* b : {&c->items, &c->info, &c->cellStart, &c->cellAtoms, &c->cellOf, &c->count, &c->fill, &c->dStart,
+                  &c->dAtoms, &c->donorMask, &c->closestH})
+    b->release();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return AG_OK;
+}
+
+extern "C" void* ag_ctx_stream(ag_ctx* c) { return c ? (void*)c->stream : nullptr; }
+extern "C" int64_t ag_ctx_launch_count(const ag_ctx* c) { return c ? c->launches : 0; }
+
+// ---------------------------------------------------------------------------
+// Job staging
+// ---------------------------------------------------------------------------
+namespace {
+
+int checkGrid(const ag_grid* g) {
+  if (!g) return fail(AG_E_INVALID, "null grid");
+  if (g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nx > 1025 || g->ny > 1025 || g->nz > 1025)
+    return fail(AG_E_INVALID, "grid %dx%dx%d outside 1..1025 points per axis", g->nx, g->ny, g->nz);
+  if (!(g->spacing > 0) || !std::isfinite(g->spacing)) return fail(AG_E_INVALID, "bad grid spacing");
+  return AG_OK;
+}
+
+// Work items of the e-map (NX points of one row each), grouped into CTAs of
+// 256 items walking 2 x 16 x 8 tiles of items, with each CTA's box.
+void buildItems(ag_ctx* c) {
+  const ag_grid& g = c->grid;
+  if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing) return;
+  const int nxc = (g.nx + agk::kNX - 1) / agk::kNX;
+  const int TX = 2, TY = 16, TZ = 8;
+  c->hItems.clear();
+  for (int tz = 0; tz < g.nz; tz += TZ)
+    for (int ty = 0; ty < g.ny; ty += TY)
+      for (int tx = 0; tx < nxc; tx += TX)
+        for (int z = tz; z < std::min(g.nz, tz + TZ); z++)
+          for (int y = ty; y < std::min(g.ny, ty + TY); y++)
+            for (int x = tx; x < std::min(nxc, tx + TX); x++) c->hItems.push_back(x | (y << 8) | (z << 19));
+  c->hBlocks.clear();
+  const double h = g.spacing;
+  const int n2x = g.nx / 2, n2y = g.ny / 2, n2z = g.nz / 2;
+  for (size_t i0 = 0; i0 < c->hItems.size(); i0 += 256) {
+    agk::EmapBlock b{};
+    b.item0 = (int)i0;
+    b.nitems = (int)std::min<size_t>(256, c->hItems.size() - i0);
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < b.nitems; k++) {
+      int v = c->hItems[i0 + k];
+      int xc = v & 0xFF, y = (v >> 8) & 0x7FF, z = (v >> 19) & 0x7FF;
+      int xa = xc * agk::kNX, xb = std::min(g.nx - 1, xa + agk::kNX - 1);
+      double p[2][3] = {{(xa - n2x) * h, (y - n2y) * h, (z - n2z) * h}, {(xb - n2x) * h, (y - n2y) * h, (z - n2z) * h}};
+      for (int q = 0; q < 2; q++)
+        for (int d = 0; d < 3; d++) {
+          lo[d] = std::min(lo[d], p[q][d]);
+          hi[d] = std::max(hi[d], p[q][d]);
+        }
+    }
+    b.ox = 0.5 * (lo[0] + hi[0]);
+    b.oy = 0.5 * (lo[1] + hi[1]);
+    b.oz = 0.5 * (lo[2] + hi[2]);
+    b.hx = (float)(50.0 * (hi[0] - lo[0]) + 1.0);
+    b.hy = (float)(50.0 * (hi[1] - lo[1]) + 1.0);
+    b.hz = (float)(50.0 * (hi[2] - lo[2]) + 1.0);
+    c->hBlocks.push_back(b);
+  }
+  c->itemsFor[0] = g.nx;
+  c->itemsFor[1] = g.ny;
+  c->itemsFor[2] = g.nz;
+  c->itemsH = g.spacing;
+}
+
+int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, bool deviceInputs) {
+  if (int r = checkGrid(g)) return r;
+  if (n < 0 || (n > 0 && !xyzw)) return fail(AG_E_INVALID, "bad atom array");
+  c->grid = *g;
+  c->nAtoms = n;
+  c->ddd = inv_eps != nullptr;
+  CK(cudaSetDevice(c->device));
+  if (!deviceInputs) {
+    for (int64_t i = 0; i < 4 * (int64_t)n; i++)
+      if (!std::isfinite(xyzw[i])) return fail(AG_E_INVALID, "non-finite atom coordinate or weight at atom %lld", (long long)(i / 4));
+    CK(c->atoms.ensure(n));
+    if (n) CK(cudaMemcpyAsync(c->atoms.p, xyzw, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+  }
+  if (c->ddd) {
+    std::vector<float> t(8192);
+    for (int i = 0; i < 8192; i++) t[i] = (float)inv_eps[i];
+    CK(c->epsTab.ensure(8192));
+    CK(cudaMemcpyAsync(c->epsTab.p, t.data(), sizeof(float) * 8192, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  buildItems(c);
+  CK(c->items.ensure(c->hItems.size()));
+  CK(c->blocks.ensure(c->hBlocks.size()));
+  CK(cudaMemcpyAsync(c->items.p, c->hItems.data(), sizeof(int) * c->hItems.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->blocks.p, c->hBlocks.data(), sizeof(agk::EmapBlock) * c->hBlocks.size(),
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return AG_OK;
+}
+
+int runEmap(ag_ctx* c, float* dOut) {
+  const int64_t np = c->npoints();
+  agk::EmapParams P{};
+  P.atoms = c->atoms.p;
+  P.n_atoms = c->nAtoms;
+  P.nblocks = (int)c->hBlocks.size();
+  P.items = c->items.p;
+  P.blocks = c->blocks.p;
+  P.nx = c->grid.nx; P.ny = c->grid.ny; P.nz = c->grid.nz;
+  P.n2x = P.nx / 2; P.n2y = P.ny / 2; P.n2z = P.nz / 2;
+  P.npoints = np;
+  P.h = c->grid.spacing;
+  P.table = c->epsTab.p;
+  P.thr = c->thr.p;
+  P.rnear2 = (100.f * c->rNear) * (100.f * c->rNear);
+  P.delta = c->delta;
+  P.out = dOut;
+  P.status = c->status.p;
+  // Split atoms across CTAs when the grid alone cannot fill the GPU.
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+  const int want = 2 * sms * 2;
+  int nsplit = 1;
+  if (P.nblocks < want && c->nAtoms > 512) nsplit = std::min((want + P.nblocks - 1) / P.nblocks, (c->nAtoms + 255) / 256);
+  int chunk = (c->nAtoms + nsplit - 1) / nsplit;
+  chunk = ((chunk + 255) / 256) * 256;
+  if (chunk == 0) chunk = 256;
+  nsplit = std::max(1, (c->nAtoms + chunk - 1) / chunk);
+  P.chunk = chunk;
+  P.nsplit = nsplit;
+  if (nsplit > 1) {
+    CK(c->partial.ensure((size_t)nsplit * np));
+    P.partial = c->partial.p;
+  }
+  if (c->nAtoms == 0) {
+    CK(cudaMemsetAsync(dOut, 0, sizeof(float) * np, c->stream));
+    return AG_OK;
+  }
+  CK(agk::emap_launch(P, c->ddd, c->emapMode, P.nblocks * nsplit, c->stream));
+  c->launches += nsplit > 1 ? 2 : 1;
+  return AG_OK;
+}
+
+int stageAffinity(ag_ctx* c, const ag_receptor* r, const ag_affinity_params* p) {
+  const int n = r->n_atoms;
+  if (p->n_maps < 0 || p->n_maps > ag::kMaxAtomTypes) return fail(AG_E_INVALID, "n_maps %d outside 0..14", p->n_maps);
+  if (p->n_types < 1 || p->n_types > ag::kNumAllTypes) return fail(AG_E_INVALID, "n_types %d outside 1..32", p->n_types);
+  std::vector<int> info(n), donor(n);
+  std::vector<float> vol(n), solq(n);
+  for (int i = 0; i < n; i++) {
+    if (r->type[i] < 0 || r->type[i] >= p->n_types) return fail(AG_E_INVALID, "atom %d has type %d outside 0..%d", i, r->type[i], p->n_types - 1);
+    if (r->hbond[i] < 0 || r->hbond[i] > 5) return fail(AG_E_INVALID, "atom %d has H-bond class %d", i, r->hbond[i]);
+    info[i] = r->type[i] | (r->hbond[i] << 5) | ((r->disorder[i] ? 1 : 0) << 8) | ((r->rexp[i] & 7) << 9);
+    donor[i] = (r->hbond[i] == ag::DS || r->hbond[i] == ag::D1) ? 1 : 0;
+    vol[i] = (float)r->vol[i];
+    solq[i] = (float)(r->solpar[i] + p->solpar_q * fabs(r->charge[i]));
+  }
+  CK(c->info.ensure(n)); CK(c->donorMask.ensure(n)); CK(c->vol.ensure(n)); CK(c->solq.ensure(n));
+  CK(c->rv.ensure(3 * (size_t)n)); CK(c->rv2.ensure(3 * (size_t)n));
+  if (n) {
+    CK(cudaMemcpyAsync(c->info.p, info.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->donorMask.p, donor.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->vol.p, vol.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->solq.p, solq.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rv.p, r->rvector, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rv2.p, r->rvector2, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  }
+  c->nMaps = p->n_maps;
+  c->nTypes = p->n_types;
+  c->hydrogen = p->hydrogen;
+  c->solparQ = p->solpar_q;
+  c->mapHbond.assign(p->map_hbond, p->map_hbond + p->n_maps);
+  c->mapIsHB.assign(p->map_is_hbonder, p->map_is_hbonder + p->n_maps);
+  c->mapCov.assign(p->map_is_covalent, p->map_is_covalent + p->n_maps);
+  c->solparProbe.assign(p->solpar_probe, p->solpar_probe + p->n_maps);
+  c->volProbe.assign(p->vol_probe, p->vol_probe + p->n_maps);
+  // Pair-energy tables, FP32, rows r <= 8 A, laid out per pass [type][row][G].
+  const int nm = p->n_maps, nt = p->n_types;
+  std::vector<float> tab((size_t)nt * agk::kAffRows * std::max(nm, 1));
+  std::vector<float> tabH((size_t)agk::kAffRows * std::max(nm, 1));
+  int G = std::max(1, std::min(nm, agk::kAffMaxGroup));
+  while (G > 1 && agk::aff_smem_bytes(nt, G) > 100 * 1024) G--;
+  int npass = nm ? (nm + G - 1) / G : 0;
+  if (npass) G = (nm + npass - 1) / npass;
+  size_t off = 0;
+  for (int m0 = 0; m0 < nm; m0 += G) {
+    int g = std::min(G, nm - m0);
+    for (int t = 0; t < nt; t++)
+      for (int i = 0; i < agk::kAffRows; i++)
+        for (int k = 0; k < g; k++)
+          tab[off + ((size_t)t * agk::kAffRows + i) * g + k] = (float)p->energy[((size_t)t * 8192 + i) * nm + m0 + k];
+    off += (size_t)nt * agk::kAffRows * g;
+  }
+  off = 0;
+  if (p->hydrogen >= 0 && p->hydrogen < nt) {
+    for (int m0 = 0; m0 < nm; m0 += G) {
+      int g = std::min(G, nm - m0);
+      for (int i = 0; i < agk::kAffRows; i++)
+        for (int k = 0; k < g; k++)
+          tabH[off + (size_t)i * g + k] = (float)p->energy[((size_t)p->hydrogen * 8192 + i) * nm + m0 + k];
+      off += (size_t)agk::kAffRows * g;
+    }
+  }
+  std::vector<float> sol(agk::kAffRows);
+  for (int i = 0; i < agk::kAffRows; i++) sol[i] = (float)p->sol[i];
+  CK(c->affTab.ensure(tab.size())); CK(c->affTabH.ensure(tabH.size())); CK(c->sol.ensure(sol.size()));
+  CK(cudaMemcpyAsync(c->affTab.p, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->affTabH.p, tabH.data(), sizeof(float) * tabH.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->sol.p, sol.data(), sizeof(float) * sol.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->haveAff = true;
+  return AG_OK;
+}
+
+int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
+  const ag_grid& g = c->grid;
+  const int64_t np = c->npoints();
+  const int n = c->nAtoms;
+  const double h = g.spacing;
+  // 8 A cells over the grid box widened by 8 A (atoms further out cannot reach a point).
+  double lo[3], hi[3];
+  const int nn[3] = {g.nx, g.ny, g.nz};
+  int ncell[3];
+  for (int d = 0; d < 3; d++) {
+    lo[d] = (double)(0 - nn[d] / 2) * h - 8.0;
+    hi[d] = (double)(nn[d] - 1 - nn[d] / 2) * h + 8.0;
+    ncell[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / 8.0));
+  }
+  const int ncellT = ncell[0] * ncell[1] * ncell[2];
+  CK(c->cellStart.ensure(ncellT + 1)); CK(c->count.ensure(ncellT + 1)); CK(c->fill.ensure(ncellT + 1));
+  CK(c->cellAtoms.ensure(n)); CK(c->cellOf.ensure(n));
+  CK(c->dStart.ensure(ncellT + 1)); CK(c->dAtoms.ensure(n));
+  CK(c->closestH.ensure(np));
+  agk::CellBuild C{};
+  C.xyz = c->atoms.p; C.n_atoms = n;
+  for (int d = 0; d < 3; d++) { C.lo[d] = lo[d]; C.ncell[d] = ncell[d]; }
+  C.cellOf = c->cellOf.p; C.count = c->count.p; C.fill = c->fill.p;
+  C.cellStart = c->cellStart.p; C.cellAtoms = c->cellAtoms.p; C.donorMask = nullptr;
+  CK(agk::cells_launch(C, ncellT, c->stream));
+  C.cellStart = c->dStart.p; C.cellAtoms = c->dAtoms.p; C.donorMask = c->donorMask.p;
+  CK(agk::cells_launch(C, ncellT, c->stream));
+  c->launches += 8;
+  agk::ClosestHParams H{};
+  H.xyz = c->atoms.p; H.cellStart = c->dStart.p; H.cellAtoms = c->dAtoms.p;
+  for (int d = 0; d < 3; d++) { H.cellLo[d] = lo[d]; H.ncell[d] = ncell[d]; }
+  H.nx = g.nx; H.ny = g.ny; H.nz = g.nz; H.n2x = g.nx / 2; H.n2y = g.ny / 2; H.n2z = g.nz / 2;
+  H.npoints = np; H.h = h; H.closestH = c->closestH.p;
+  CK(agk::closest_h_launch(H, c->stream));
+  c->launches += 1;
+
+  const int nm = c->nMaps, nt = c->nTypes;
+  int G = std::max(1, std::min(nm, agk::kAffMaxGroup));
+  while (G > 1 && agk::aff_smem_bytes(nt, G) > 100 * 1024) G--;
+  int npass = nm ? (nm + G - 1) / G : 0;
+  if (npass) G = (nm + npass - 1) / npass;
+  size_t off = 0, offH = 0;
+  for (int m0 = 0, pass = 0; m0 < nm || (nm == 0 && pass == 0); m0 += std::max(G, 1), pass++) {
+    const int gsz = nm ? std::min(G, nm - m0) : 0;
+    agk::AffParams P{};
+    P.n_atoms = n; P.xyz = c->atoms.p; P.info = c->info.p; P.vol = c->vol.p; P.solq = c->solq.p;
+    P.rv = c->rv.p; P.rv2 = c->rv2.p;
+    P.cellStart = c->cellStart.p; P.cellAtoms = c->cellAtoms.p;
+    for (int d = 0; d < 3; d++) { P.cellLo[d] = lo[d]; P.ncell[d] = ncell[d]; }
+    P.closestH = c->closestH.p;
+    P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.n2x = g.nx / 2; P.n2y = g.ny / 2; P.n2z = g.nz / 2;
+    P.npoints = np; P.h = h;
+    P.m0 = m0; P.G = gsz; P.nmaps = nm; P.ntypes = nt; P.hydrogen = c->hydrogen; P.doDmap = pass == 0;
+    P.table = c->affTab.p + off;
+    P.tableH = (c->hydrogen >= 0 && c->hydrogen < nt) ? c->affTabH.p + offH : nullptr;
+    P.sol = c->sol.p;
+    for (int k = 0; k < gsz; k++) {
+      P.mapHbond[k] = c->mapHbond[m0 + k];
+      P.mapIsHB[k] = c->mapIsHB[m0 + k];
+      P.mapCov[k] = c->mapCov[m0 + k];
+      P.solparProbe[k] = c->solparProbe[m0 + k];
+      P.volProbe[k] = c->volProbe[m0 + k];
+    }
+    P.solparQ = (float)c->solparQ;
+    P.out = dMaps;
+    P.dmap = dDmap;
+    P.status = c->status.p;
+    CK(agk::aff_launch(P, c->stream));
+    c->launches += 1;
+    off += (size_t)nt * agk::kAffRows * gsz;
+    offH += (size_t)agk::kAffRows * gsz;
+    if (nm == 0) break;
+  }
+  return AG_OK;
+}
+
+int checkStatus(ag_ctx* c) {
+  unsigned st = 0;
+  CK(cudaMemcpyAsync(&st, c->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), c->stream);
+    cudaStreamSynchronize(c->stream);
+    return fail(AG_E_DEVICE, "a kernel reported error status 0x%x (1 = bounded wait expired, 2 = bad input)", st);
+  }
+  return AG_OK;
+}
+
+}  // namespace
+
+extern "C" int ag_upload(ag_ctx* c, const ag_grid* g, const ag_receptor* r, const ag_affinity_params* p,
+                         const double* inv_eps) {
+  if (!c || !r) return fail(AG_E_INVALID, "null argument");
+  c->haveJob = false;
+  c->haveAff = false;
+  if (int e = stageEmap(c, g, r->n_atoms, r->xyzw, inv_eps, false)) return e;
+  c->nMaps = 0;
+  if (p)
+    if (int e = stageAffinity(c, r, p)) return e;
+  CK(c->maps.ensure((size_t)(c->nMaps + 2) * c->npoints()));
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), c->stream));
+  c->haveJob = true;
+  return AG_OK;
+}
+
+extern "C" int ag_compute(ag_ctx* c, int work) {
+  if (!c || !c->haveJob) return fail(AG_E_INVALID, "no job uploaded");
+  CK(cudaSetDevice(c->device));
+  const int64_t np = c->npoints();
+  float* maps = c->maps.p;
+  if (work & AG_WORK_EMAP)
+    if (int e = runEmap(c, maps + (size_t)c->nMaps * np)) return e;
+  if ((work & AG_WORK_AFFINITY) && c->haveAff)
+    if (int e = runAffinity(c, maps, maps + (size_t)(c->nMaps + 1) * np)) return e;
+  CK(cudaGetLastError());
+  return AG_OK;
+}
+
+extern "C" float* ag_device_maps(ag_ctx* c) { return c ? c->maps.p : nullptr; }
+
+extern "C" int ag_download(ag_ctx* c, float* out) {
+  if (!c || !c->haveJob || !out) return fail(AG_E_INVALID, "nothing to download");
+  CK(cudaMemcpyAsync(out, c->maps.p, sizeof(float) * (size_t)(c->nMaps + 2) * c->npoints(), cudaMemcpyDeviceToHost,
+                     c->stream));
+  return checkStatus(c);
+}
+
+extern "C" int ag_emap_mode(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, int mode,
+                            float* out) {
+  if (!c || !out) return fail(AG_E_INVALID, "null argument");
+  if (mode != AG_EMAP_KAHAN && mode != AG_EMAP_PLAIN) return fail(AG_E_INVALID, "unknown e-map mode %d", mode);
+  c->haveJob = false;
+  c->haveAff = false;
+  c->nMaps = 0;
+  if (int e = stageEmap(c, g, n, xyzw, inv_eps, false)) return e;
+  CK(c->maps.ensure((size_t)2 * c->npoints()));
+  c->emapMode = mode;
+  int e = runEmap(c, c->maps.p);
+  c->emapMode = agk::kEmapKahan;
+  if (e) return e;
+  CK(cudaMemcpyAsync(out, c->maps.p, sizeof(float) * c->npoints(), cudaMemcpyDeviceToHost, c->stream));
+  return checkStatus(c);
+}
+
+extern "C" int ag_emap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, float* out) {
+  return ag_emap_mode(c, g, n, xyzw, inv_eps, AG_EMAP_KAHAN, out);
+}
+
+extern "C" int ag_affinity(ag_ctx* c, const ag_grid* g, const ag_receptor* r, const ag_affinity_params* p,
+                           float* out_maps, float* out_dmap) {
+  if (!c || !r || !p || !out_dmap || (p->n_maps > 0 && !out_maps)) return fail(AG_E_INVALID, "null argument");
+  if (int e = ag_upload(c, g, r, p, nullptr)) return e;
+  if (int e = ag_compute(c, AG_WORK_AFFINITY)) return e;
+  const int64_t np = c->npoints();
+  if (p->n_maps)
+    CK(cudaMemcpyAsync(out_maps, c->maps.p, sizeof(float) * p->n_maps * np, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(out_dmap, c->maps.p + (size_t)(p->n_maps + 1) * np, sizeof(float) * np, cudaMemcpyDeviceToHost,
+                     c->stream));
+  return checkStatus(c);
+}
+
+// ---------------------------------------------------------------------------
+// Whole jobs
+// ---------------------------------------------------------------------------
+struct ag_problem {
+  ag::Problem p;
+  std::unique_ptr<ag::ParamLib> lib;
+  ag::Log log;
+  std::vector<int> mapHbond, mapIsHB, mapCov;
+  std::vector<double> solparProbe, volProbe;
+};
+
+extern "C" int ag_problem_load(const char* gpf, int v4, const char* log_path, ag_problem** out) {
+  if (!out) return fail(AG_E_INVALID, "null output pointer");
+  auto* P = new ag_problem();
+  try {
+    P->log.open(log_path);
+    P->lib.reset(new ag::ParamLib(v4 != 0));
+    ag::loadGPF(P->p, *P->lib, P->log, gpf);
+    ag::precompute(P->p, *P->lib, P->log);
+  } catch (ag::ExitProgram& e) {
+    delete P;
+    return fail(AG_E_HOST, "exit %d: %s", e.code, e.msg.c_str());
+  }
+  for (auto& m : P->p.maps) {
+    P->mapHbond.push_back(m.hbond);
+    P->mapIsHB.push_back(m.isHBonder ? 1 : 0);
+    P->mapCov.push_back(m.isCovalent ? 1 : 0);
+    P->solparProbe.push_back(m.solparProbe);
+    P->volProbe.push_back(m.volProbe);
+  }
+  *out = P;
+  return AG_OK;
+}
+
+extern "C" void ag_problem_free(ag_problem* p) { delete p; }
+
+extern "C" int ag_problem_info_get(const ag_problem* P, ag_problem_info* info) {
+  if (!P || !info) return fail(AG_E_INVALID, "null argument");
+  const ag::Problem& p = P->p;
+  info->nx = p.n[0]; info->ny = p.n[1]; info->nz = p.n[2];
+  info->spacing = p.spacing;
+  for (int k = 0; k < 3; k++) info->center[k] = p.center[k];
+  info->n_atoms = p.numAtoms;
+  info->n_maps = p.numMaps();
+  info->n_types = p.numReceptorTypes;
+  info->dist_dep_diel = p.distDepDiel;
+  info->has_floating_grid = p.hasFloatingGrid();
+  return AG_OK;
+}
+
+extern "C" int ag_problem_views(const ag_problem* P, ag_grid* g, ag_receptor* r, ag_affinity_params* a,
+                                const double** inv_eps) {
+  if (!P) return fail(AG_E_INVALID, "null problem");
+  const ag::Problem& p = P->p;
+  if (g) { g->nx = p.n[0]; g->ny = p.n[1]; g->nz = p.n[2]; g->spacing = p.spacing; }
+  if (r) {
+    r->n_atoms = p.numAtoms;
+    r->xyzw = p.xyzw.data();
+    r->charge = p.charge.data(); r->vol = p.vol.data(); r->solpar = p.solpar.data();
+    r->type = p.atomType.data(); r->hbond = p.hbond.data();
+    r->disorder = p.disorder.data(); r->rexp = p.rexp.data();
+    r->rvector = p.rvector.data(); r->rvector2 = p.rvector2.data();
+  }
+  if (a) {
+    a->n_maps = p.numMaps();
+    a->n_types = std::max(1, p.numReceptorTypes);
+    a->energy = p.energy.data();
+    a->sol = p.sol.data();
+    a->map_hbond = P->mapHbond.data();
+    a->map_is_hbonder = P->mapIsHB.data();
+    a->map_is_covalent = P->mapCov.data();
+    a->solpar_probe = P->solparProbe.data();
+    a->vol_probe = P->volProbe.data();
+    a->solpar_q = p.solparQ;
+    a->hydrogen = p.hydrogen;
+  }
+  if (inv_eps) *inv_eps = p.distDepDiel ? p.epsilon.data() : nullptr;
+  return AG_OK;
+}
+
+extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
+  if (!c || !P) return fail(AG_E_INVALID, "null argument");
+  ag::Problem& p = P->p;
+  ag_grid g;
+  ag_receptor r;
+  ag_affinity_params a;
+  const double* eps = nullptr;
+  ag_problem_views(P, &g, &r, &a, &eps);
+  if (int e = ag_upload(c, &g, &r, &a, eps)) return e;
+  if (int e = ag_compute(c, AG_WORK_ALL)) return e;
+  const int64_t np = c->npoints();
+  for (int m = 0; m < p.numMaps(); m++)
+    if (p.maps[m].isCovalent) {
+      CK(agk::covalent_launch(c->maps.p + (size_t)m * np, g.nx, g.ny, g.nz, g.spacing, p.covalentPoint,
+                              p.covHalfWidthSquaredInv, p.covBarrier, c->stream));
+      c->launches++;
+    }
+  p.out.resize((size_t)(p.numMaps() + 2) * np);
+  if (int e = ag_download(c, p.out.data())) return e;
+  if (p.hasFloatingGrid()) {
+    DevBuf<float> fg;
+    CK(fg.ensure(np));
+    CK(agk::floating_launch(c->atoms.p, p.numAtoms, g.nx, g.ny, g.nz, g.spacing, fg.p, c->stream));
+    c->launches++;
+    p.floatingGrid.resize(np);
+    CK(cudaMemcpyAsync(p.floatingGrid.data(), fg.p, sizeof(float) * np, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    fg.release();
+  }
+  return AG_OK;
+}
+
+extern "C" const float* ag_problem_maps(const ag_problem* P) { return P && !P->p.out.empty() ? P->p.out.data() : nullptr; }
+
+extern "C" int ag_problem_write(ag_problem* P) {
+  if (!P || P->p.out.empty()) return fail(AG_E_INVALID, "no computed maps");
+  try {
+    for (int m = 0; m < P->p.numMaps() + 2; m++) ag::writeMap(P->p, m, P->log);
+    ag::writeFloatingGrid(P->p, P->log);
+  } catch (ag::ExitProgram& e) {
+    return fail(AG_E_HOST, "exit %d: %s", e.code, e.msg.c_str());
+  }
+  return AG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Command line (ProgramParameters.cpp:63-112, main.cpp:115-279)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Timer {
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double ms() const { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+void printHelp(const char* prog) {
+  fprintf(stderr,
+          "Usage: %s [OPTIONS]\n\n"
+          "Stream control:\n"
+          "  -l, --log FILE    log to FILE, default: standard output\n"
+          "  -p, --gpf FILE    read grid parameters from FILE, default: standard input\n\n"
+          "Miscellaneous:\n"
+          "      --benchmark   print execution times to standard error output\n"
+          "      --cuda-enum   enumerate all CUDA devices and exit\n"
+          "      --cuda-dev N  use a CUDA device number N, default: 0\n"
+          "  -d, --debug       increment debug level\n"
+          "  -u, --help        display this help and exit\n"
+          "      --timeout N   terminate if calculations does not finish in N seconds\n"
+          "      --v4          set the AutoGrid 4.0 default parameter library\n\n"
+          "Accepted for compatibility and ignored (the maps are always computed on the GPU):\n"
+          "      --no-cuda --omp N --cogrid-mem N --no-cogrid --no-nns\n"
+          "      --cuda-ddd=g|c|t|i --cuda-slices=y|n --cuda-thread=y|n --cuda-unroll=y|n\n",
+          prog);
+}
+
+int runMain(int argc, char** argv) {
+  const char* prog = argv[0];
+  std::string gpf, logf;
+  bool bench = false, v4 = false;
+  int dev = 0;
+  for (int i = 1; i < argc; i++) {
+    std::string a = argv[i];
+    auto needArg = [&](void) -> const char* {
+      if (i + 1 >= argc) throw ag::ExitProgram{1, "missing argument for " + a};
+      return argv[++i];
+    };
+    auto needInt = [&](void) -> int {
+      const char* s = needArg();
+      int v;
+      if (sscanf(s, "%i", &v) != 1) {
+        fprintf(stderr, "%s: '%s' is not a number\n", prog, s);
+        throw ag::ExitProgram{1, "not a number"};
+      }
+      return v;
+    };
+    if (a == "-l" || a == "--log") logf = needArg();
+    else if (a == "-p" || a == "--gpf") gpf = needArg();
+    else if (a == "--benchmark") bench = true;
+    else if (a == "--cogrid-mem" || a == "--omp") needInt();
+    else if (a == "--cuda-enum") {
+      int n = 0;
+      cudaGetDeviceCount(&n);
+      fprintf(stderr, "Found %i CUDA devices:\n\n # | Name                           | MPs | Cap | GlobalMem\n", n);
+      for (int d = 0; d < n; d++) {
+        cudaDeviceProp pr;
+        cudaGetDeviceProperties(&pr, d);
+        fprintf(stderr, "%2i | %-31s|%4i |%2i.%-2i|%6lu MiB\n", d, pr.name, pr.multiProcessorCount, pr.major, pr.minor,
+                (unsigned long)(pr.totalGlobalMem >> 20));
+      }
+      return 0;
+    } else if (a == "--cuda-dev") dev = needInt();
+    else if (a == "-d" || a == "--debug") {}
+    else if (a == "-u" || a == "--help") { printHelp(prog); return 0; }
+    else if (a == "--no-cuda" || a == "--no-cogrid" || a == "--no-nns" || a.rfind("--cuda-ddd=", 0) == 0 ||
+             a.rfind("--cuda-slices=", 0) == 0 || a.rfind("--cuda-thread=", 0) == 0 || a.rfind("--cuda-unroll=", 0) == 0) {}
+    else if (a == "--timeout") {
+      int secs = needInt();
+      pid_t pid = fork();
+      if (pid > 0) {
+        int status = 0;
+        for (int t = 0; t < secs * 10; t++) {
+          if (waitpid(pid, &status, WNOHANG) == pid) return 0;
+          usleep(100000);
+        }
+        kill(pid, SIGKILL);
+        waitpid(pid, &status, 0);
+        fprintf(stderr, "Timeout! Process terminated.\n");
+        return 0;
+      }
+    } else if (a == "--v4") v4 = true;
+    else {
+      fprintf(stderr, "%s: unknown switch '%s'\n", prog, a.c_str());
+      return 1;
+    }
+  }
+
+  Timer total;
+  ag::Problem p;
+  ag::Log log;
+  log.programName = prog;
+  log.open(logf.c_str());
+  log.print("%s 4.2.1 (B200 map engine)\n\n", prog);
+  ag::ParamLib lib(v4);
+  Timer t0;
+  ag::loadGPF(p, lib, log, gpf.empty() ? nullptr : gpf.c_str());
+  ag::precompute(p, lib, log);
+  ag::writeFld(p, prog, log);
+  if (bench) fprintf(stderr, "Precalculations          Real: %.0f ms\n", t0.ms());
+
+  ag_ctx* ctx = nullptr;
+  if (ag_ctx_create(dev, &ctx) != AG_OK) log.fatal(-2, "%s", ag_last_error());
+  ag_problem P;
+  P.p = std::move(p);
+  for (auto& m : P.p.maps) {
+    P.mapHbond.push_back(m.hbond);
+    P.mapIsHB.push_back(m.isHBonder ? 1 : 0);
+    P.mapCov.push_back(m.isCovalent ? 1 : 0);
+    P.solparProbe.push_back(m.solparProbe);
+    P.volProbe.push_back(m.volProbe);
+  }
+  Timer t1;
+  if (ag_problem_compute(ctx, &P) != AG_OK) {
+    std::string e = ag_last_error();
+    ag_ctx_destroy(ctx);
+    log.fatal(-2, "%s", e.c_str());
+  }
+  const double gpuMs = t1.ms();
+  ag_ctx_destroy(ctx);
+  if (bench) {
+    fprintf(stderr, "Grid maps (GPU)          Real: %.0f ms\n", gpuMs);
+    double pairs = (double)P.p.numAtoms * (double)P.p.numPoints;
+    fprintf(stderr, "Electrostatics performance: %i million atoms/s (whole map set)\n", (int)(pairs / (gpuMs * 1e-3) / 1e6));
+  }
+  Timer t2;
+  for (int m = 0; m < P.p.numMaps() + 2; m++) ag::writeMap(P.p, m, log);
+  ag::writeFloatingGrid(P.p, log);
+  if (bench) fprintf(stderr, "Saving maps              Real: %.0f ms\n", t2.ms());
+
+  // Summary of extrema (GridMap.cpp:53-82), over the rounded values.
+  log.print("\nGrid\tAtom\tMinimum   \tMaximum\nMap \tType\tEnergy    \tEnergy \n\t\t(kcal/mol)\t(kcal/mol)\n____\t____\t_____________\t_____________\n");
+  const int64_t np = P.p.numPoints;
+  for (int m = 0; m < P.p.numMaps() + 2; m++) {
+    double mn = ag::kBig, mx = -ag::kBig;
+    for (int64_t j = 0; j < np; j++) {
+      double v = ag::roundOutput(P.p.out[(size_t)m * np + j]);
+      mn = std::min(mn, v);
+      mx = std::max(mx, v);
+    }
+    const char* type = m < P.p.numMaps() ? P.p.maps[m].type : (m == P.p.numMaps() ? "e" : "d");
+    log.print(" %d\t %s\t  %6.2lf\t%9.2le\n", m + 1, type, mn, mx);
+  }
+  log.print("\n\n * Note:  Every pairwise-atomic interaction was clamped at %.2f\n\n\n", ag::kEintClamp);
+  fprintf(stderr, "\n%s: Successful Completion.\n", prog);
+  log.print("%s: Successful Completion.\n", prog);
+  if (bench) fprintf(stderr, "Total                    Real: %.0f ms\n", total.ms());
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int ag_main(int argc, char** argv) {
+  try {
+    return runMain(argc, argv);
+  } catch (ag::ExitProgram& e) {
+    return e.code;
+  } catch (std::bad_alloc&) {
+    fprintf(stderr, "\n%s: FATAL ERROR: Not enough memory!\n", argv[0]);
+    return (int)0xBADA110C;
+  }
+}

@@ -1,0 +1,304 @@
+// Electrostatic map (e-map) by direct summation over all receptor atoms.
+//
+//   e(p) = sum_a w_a * min(1/r, 2) * invEps[min(int(100 r), 8191)]
+//
+// (FastGrid electrostatics/Cpu.cpp:27-88; the table is InputDataLoader.cpp:
+// 715-742).  There is no cutoff, so the work is N_atoms x N_points pairs and
+// the kernel is bound by the SM's issue rate (one SFU rsqrt, one shared-memory
+// table read and ~10 FP32 ops per pair), not by HBM.
+//
+// Layout and schedule
+//  * Work item = NX consecutive x points of one (y, z) row; one thread per item,
+//    256 items per CTA, items grouped by the host into compact boxes.
+//  * Atoms stream through shared memory in tiles of kTile FP64 (x, y, z, w)
+//    records, fetched with 1-D TMA bulk copies into a two-slot ring and
+//    tracked by mbarriers (no multicast).
+//  * Each tile is converted once per CTA to CTA-local coordinates scaled by
+//    100 (so 100*r comes straight out of r^2 * rsqrt(r^2)) and split into
+//    "near" atoms (closer than rNear to the CTA's box) and "far" atoms.
+//  * Far pairs: floor(100 r) by a round-toward-minus-infinity FMA, table read
+//    from shared memory, Kahan-compensated FP32 sum.
+//  * Near pairs additionally clamp 1/r at 2 and check whether 100 r lies within
+//    `delta` of a bin edge; if so the bin is decided exactly in FP64 against
+//    a table of squared-distance thresholds, so the step-function table is
+//    indexed exactly as the reference's FP64 code indexes it.
+//  * Tile sums are added into per-point FP64 accumulators.  When the grid is
+//    too small to fill the GPU, atoms are split across CTAs and the FP64
+//    partial sums are reduced in a fixed order by a second kernel.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ag_device.cuh"
+#include "ag_kernels.h"
+
+namespace agk {
+
+using namespace agd;
+
+constexpr int kThreads = 256;
+constexpr int kTile = 256;        // atoms per shared-memory tile
+constexpr int kTabLen = 8192;     // invEps entries
+
+struct EmapSmem {
+  float tab[kTabLen];             // 32 KB
+  double4 ring[2][kTile];         // 16 KB, TMA destination
+  float4 nearA[kTile];            // local scaled x, y, z and 100*w
+  float4 farA[kTile];
+  short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
+  int cnt[2][kThreads / 32];
+  uint64_t bar[2];
+};
+
+__device__ __forceinline__ void unpack_item(int v, int& xc, int& y, int& z) {
+  xc = v & 0xFF;
+  y = (v >> 8) & 0x7FF;
+  z = (v >> 19) & 0x7FF;
+}
+
+template <bool DDD, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int blk = blockIdx.x % P.nblocks, split = blockIdx.x / P.nblocks;
+  const EmapBlock B = P.blocks[blk];
+  const int a0 = split * P.chunk;
+  const int a1 = min(P.n_atoms, a0 + P.chunk);
+  const int ntiles = (a1 - a0 + kTile - 1) / kTile;
+
+  // This thread's points, in the CTA-local frame scaled by 100.
+  const bool active = tid < B.nitems;
+  int xc = 0, iy = 0, iz = 0;
+  unpack_item(P.items[B.item0 + (active ? tid : 0)], xc, iy, iz);
+  const double h = P.h;
+  float gx[kNX];
+#pragma unroll
+  for (int k = 0; k < kNX; k++)
+    gx[k] = (float)(((double)(xc * kNX + k - P.n2x) * h - B.ox) * 100.0);
+  const float gy = (float)(((double)(iy - P.n2y) * h - B.oy) * 100.0);
+  const float gz = (float)(((double)(iz - P.n2z) * h - B.oz) * 100.0);
+
+  if (DDD) {
+    const float4* src = reinterpret_cast<const float4*>(P.table);
+    float4* dst = reinterpret_cast<float4*>(S.tab);
+    for (int i = tid; i < kTabLen / 4; i += kThreads) dst[i] = src[i];
+  }
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (tid == 0 && ntiles > 0) {
+    unsigned n0 = (unsigned)min(kTile, a1 - a0);
+    mbar_arrive_expect_tx(&S.bar[0], n0 * 32u);
+    tma_load_1d(S.ring[0], P.atoms + a0, n0 * 32u, &S.bar[0]);
+  }
+
+  double acc[kNX];
+  float sum[kNX], cmp[kNX];
+#pragma unroll
+  for (int k = 0; k < kNX; k++) { acc[k] = 0.0; sum[k] = 0.f; cmp[k] = 0.f; }
+
+  const float cap = 0.02f;  // min(1/r, 2) in units of 1/(100 r)
+  const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
+
+  for (int t = 0; t < ntiles; t++) {
+    const int slot = t & 1;
+    const int t0 = a0 + t * kTile;
+    const int nt = min(kTile, a1 - t0);
+    if (tid == 0 && t + 1 < ntiles) {
+      // The other slot was released by the __syncthreads() that ended tile t-1.
+      const int t1 = t0 + kTile;
+      unsigned n1 = (unsigned)min(kTile, a1 - t1);
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&S.bar[slot ^ 1], n1 * 32u);
+      tma_load_1d(S.ring[slot ^ 1], P.atoms + t1, n1 * 32u, &S.bar[slot ^ 1]);
+    }
+    bool ok = mbar_wait_bounded(&S.bar[slot], (unsigned)(t >> 1) & 1u, P.status);
+    if (__syncthreads_or(!ok)) return;
+
+    // Classify and convert this tile's atoms (one atom per thread).
+    bool isNear = false;
+    float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool have = tid < nt;
+    if (have) {
+      double4 a = S.ring[slot][tid];
+      loc.x = (float)((a.x - B.ox) * 100.0);
+      loc.y = (float)((a.y - B.oy) * 100.0);
+      loc.z = (float)((a.z - B.oz) * 100.0);
+      loc.w = (float)(a.w * 100.0);
+      float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
+            dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
+      isNear = dx * dx + dy * dy + dz * dz < P.rnear2;
+    }
+    const unsigned nb = __ballot_sync(0xffffffffu, have && isNear);
+    const unsigned fb = __ballot_sync(0xffffffffu, have && !isNear);
+    if (lane == 0) { S.cnt[0][warp] = __popc(nb); S.cnt[1][warp] = __popc(fb); }
+    __syncthreads();
+    int nNear = 0, nFar = 0, offN = 0, offF = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; w++) {
+      if (w == warp) { offN = nNear; offF = nFar; }
+      nNear += S.cnt[0][w];
+      nFar += S.cnt[1][w];
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    if (have) {
+      if (isNear) {
+        int pos = offN + __popc(nb & lt);
+        S.nearA[pos] = loc;
+        S.nearIdx[pos] = (short)tid;
+      } else {
+        S.farA[offF + __popc(fb & lt)] = loc;
+      }
+    }
+    __syncthreads();
+
+    // Far atoms.
+#pragma unroll 1
+    for (int j = 0; j < nFar; j++) {
+      const float4 a = S.farA[j];
+      const float dy = a.y - gy, dz = a.z - gz;
+      const float dyz2 = fmaf(dz, dz, dy * dy);
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        const float dx = a.x - gx[k];
+        const float r2 = fmaf(dx, dx, dyz2);
+        const float rs = rsqrt_approx(r2);
+        float term;
+        if (DDD) {
+          float f = __fmaf_rd(r2, rs, kBias);
+          f = fminf(f, kBias + (float)(kTabLen - 1));
+          term = (a.w * rs) * S.tab[__float_as_int(f) - 0x4B000000];
+        } else {
+          term = a.w * rs;
+        }
+        if (MODE == kEmapKahan) {
+          const float y = term - cmp[k];
+          const float s1 = sum[k] + y;
+          cmp[k] = (s1 - sum[k]) - y;
+          sum[k] = s1;
+        } else {
+          sum[k] += term;
+        }
+      }
+    }
+
+    // Near atoms: clamp 1/r at 2 and decide bins near an edge exactly.
+#pragma unroll 1
+    for (int j = 0; j < nNear; j++) {
+      const float4 a = S.nearA[j];
+      const float dy = a.y - gy, dz = a.z - gz;
+      const float dyz2 = fmaf(dz, dz, dy * dy);
+      float rsv[kNX];
+      int idx[kNX];
+      int kmid[kNX];
+      unsigned flags = 0;
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        const float dx = a.x - gx[k];
+        const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
+        const float rs = rsqrt_approx(r2);
+        rsv[k] = rs;
+        if (DDD) {
+          const float T = r2 * rs;
+          float f = __fmaf_rd(r2, rs, kBias);
+          f = fminf(f, kBias + (float)(kTabLen - 1));
+          idx[k] = __float_as_int(f) - 0x4B000000;
+          const float kr = (T + 12582912.f) - 12582912.f;  // nearest integer (T < 2^22)
+          kmid[k] = (int)kr;
+          if (fabsf(T - kr) < P.delta && kr >= 1.f && kr < (float)kTabLen) flags |= 1u << k;
+        }
+      }
+      if (DDD && __any_sync(0xffffffffu, flags != 0)) {
+        if (flags) {
+          const double4 a64 = S.ring[slot][S.nearIdx[j]];
+          const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
+          const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
+          const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
+#pragma unroll
+          for (int k = 0; k < kNX; k++) {
+            if (flags & (1u << k)) {
+              const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
+              const double ddx = __dsub_rn(a64.x, gx64);
+              const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
+              idx[k] = (r2d >= P.thr[kmid[k]]) ? kmid[k] : kmid[k] - 1;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        const float c = fminf(rsv[k], cap);
+        const float term = DDD ? (a.w * c) * S.tab[idx[k]] : a.w * c;
+        if (MODE == kEmapKahan) {
+          const float y = term - cmp[k];
+          const float s1 = sum[k] + y;
+          cmp[k] = (s1 - sum[k]) - y;
+          sum[k] = s1;
+        } else {
+          sum[k] += term;
+        }
+      }
+    }
+
+    if (MODE == kEmapKahan) {
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        acc[k] += (double)sum[k] - (double)cmp[k];
+        sum[k] = 0.f;
+        cmp[k] = 0.f;
+      }
+    }
+    __syncthreads();  // ring slot and atom lists are free again
+  }
+
+  if (!active) return;
+  const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;
+#pragma unroll
+  for (int k = 0; k < kNX; k++) {
+    const int x = xc * kNX + k;
+    if (x >= P.nx) break;
+    const double v = (MODE == kEmapKahan) ? acc[k] : (double)sum[k];
+    if (P.nsplit == 1)
+      P.out[row + x] = (float)v;
+    else
+      P.partial[(int64_t)split * P.npoints + row + x] = v;
+  }
+}
+
+// Sum the atom-split partials in split order.
+__global__ void emap_reduce_kernel(const double* __restrict__ partial, int nsplit, int64_t n, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < nsplit; k++) s += partial[(int64_t)k * n + i];
+    out[i] = (float)s;
+  }
+}
+
+size_t emap_smem_bytes() { return sizeof(EmapSmem); }
+
+cudaError_t emap_launch(const EmapParams& P, bool ddd, int mode, int grid, cudaStream_t st) {
+  const size_t smem = sizeof(EmapSmem);
+  cudaError_t e = cudaSuccess;
+#define AG_LAUNCH(D, M)                                                                               \
+  do {                                                                                                \
+    e = cudaFuncSetAttribute(emap_kernel<D, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (e != cudaSuccess) return e;                                                                   \
+    emap_kernel<D, M><<<grid, kThreads, smem, st>>>(P);                                               \
+  } while (0)
+  if (ddd) {
+    if (mode == kEmapKahan) AG_LAUNCH(true, kEmapKahan); else AG_LAUNCH(true, kEmapPlain);
+  } else {
+    if (mode == kEmapKahan) AG_LAUNCH(false, kEmapKahan); else AG_LAUNCH(false, kEmapPlain);
+  }
+#undef AG_LAUNCH
+  e = cudaGetLastError();
+  if (e != cudaSuccess || P.nsplit == 1) return e;
+  emap_reduce_kernel<<<592, 256, 0, st>>>(P.partial, P.nsplit, P.npoints, P.out);
+  return cudaGetLastError();
+}
+
+}  // namespace agk

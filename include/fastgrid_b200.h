@@ -1,0 +1,189 @@
+/*
+ * fastgrid_b200 — C ABI of the B200 AutoGrid grid-map engine.
+ *
+ * The engine computes an AutoGrid map set on one GPU: the electrostatic map
+ * (e-map), one affinity map per ligand atom type and the desolvation map
+ * (d-map).  The entry points below are the seams at which the reference
+ * (FastGrid, fastgrid_master/fastgrid/) dispatches that work; each declaration
+ * names the reference interface it replaces.  All arguments are plain C types
+ * and host pointers unless a name says "device"; no exceptions cross this
+ * boundary.  Every function returns AG_OK (0) or a negative AG_E* code, and
+ * ag_last_error() then describes the failure (thread-local).
+ *
+ * Coordinates are in the grid-centred frame used by the reference: grid point
+ * (i, j, k) sits at ((i - nx/2)*h, (j - ny/2)*h, (k - nz/2)*h) with integer
+ * division (autogrid.h:267-286), and receptor atoms have had the grid centre
+ * subtracted (InputDataLoader.cpp:466-467).  Map values are written x fastest,
+ * then y, then z, as FP32 and unrounded (the writers round to 3 decimals).
+ */
+#ifndef FASTGRID_B200_H
+#define FASTGRID_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AG_OK 0
+#define AG_E_INVALID (-1)   /* bad argument */
+#define AG_E_CUDA (-2)      /* CUDA runtime error (device, launch, copy) */
+#define AG_E_DEVICE (-3)    /* a kernel reported an error status (e.g. a bounded wait expired) */
+#define AG_E_HOST (-4)      /* input file / host-side failure */
+#define AG_E_NOMEM (-5)     /* allocation failure */
+
+#define AG_TABLE_LEN 8192   /* 0.01 A bins, MAX_DIST (autogrid.h:215) */
+
+typedef struct ag_ctx ag_ctx;
+typedef struct ag_problem ag_problem;
+
+/* Grid shape: nx, ny, nz points (odd in AutoGrid GPFs) at `spacing` A. */
+typedef struct ag_grid {
+  int nx, ny, nz;
+  double spacing;
+} ag_grid;
+
+/* Receptor, structure of arrays (InputData.h:53-58 + BondVectors.h:27-31). */
+typedef struct ag_receptor {
+  int n_atoms;
+  const double* xyzw;          /* 4 per atom: centred x, y, z and the e-map weight
+                                  q*coeff_estat (distance-dependent dielectric) or
+                                  q*coeff_estat*332/diel (constant dielectric) */
+  const double* charge;        /* partial charge q */
+  const double* vol;           /* atomic fragmental volume */
+  const double* solpar;        /* atomic solvation parameter */
+  const int* type;             /* receptor type index, < n_types */
+  const int* hbond;            /* 0 NON, 1 DS, 2 D1, 3 AS, 4 A1, 5 A2 */
+  const unsigned char* disorder;
+  const int* rexp;             /* 2 (N-H) or 4 (O-H / S-H) for D1 atoms */
+  const double* rvector;       /* 3 per atom, unit bond vector */
+  const double* rvector2;      /* 3 per atom, unit lone-pair plane normal (A2) */
+} ag_receptor;
+
+/* Per-map parameters of the affinity + desolvation pass
+ * (GridMap.h:27-57, PairwiseInteractionEnergies.h:31-49, DesolvExpFunc.h). */
+typedef struct ag_affinity_params {
+  int n_maps;                  /* ligand (atom) maps, <= 14 */
+  int n_types;                 /* receptor types, <= 32 */
+  const double* energy;        /* [n_types][AG_TABLE_LEN][n_maps] pair energies */
+  const double* sol;           /* [AG_TABLE_LEN] coeff_desolv*exp(-r^2/25.92) */
+  const int* map_hbond;        /* per map: H-bond character of the probe */
+  const int* map_is_hbonder;   /* per map: GridMap::isHBonder */
+  const int* map_is_covalent;  /* per map: covalent maps are skipped here */
+  const double* solpar_probe;  /* per map */
+  const double* vol_probe;     /* per map */
+  double solpar_q;             /* charge-dependent solvation coefficient (qasp) */
+  int hydrogen;                /* receptor type index of "HD", or -1 */
+} ag_affinity_params;
+
+/* ------------------------------------------------------------------------ */
+/* Context: one per host thread; owns a CUDA stream and device buffers.     */
+/* ------------------------------------------------------------------------ */
+int ag_ctx_create(int device, ag_ctx** out);
+int ag_ctx_destroy(ag_ctx* ctx);
+const char* ag_last_error(void);
+/* The cudaStream_t the context launches on (for event timing by callers). */
+void* ag_ctx_stream(ag_ctx* ctx);
+/* Number of kernel launches issued by this context so far. */
+int64_t ag_ctx_launch_count(const ag_ctx* ctx);
+
+/* ------------------------------------------------------------------------ */
+/* Electrostatic map.                                                        */
+/* Replaces calculateElectrostaticMapAsync + synchronizeCalculation          */
+/* (electrostatics/Electrostatics.h:32-36; CPU body Cpu.cpp:27-112, CUDA     */
+/* body Cuda.cpp:75-249).  e(p) = sum over all atoms of                       */
+/* w * min(1/r, 2) * inv_eps[min(int(100 r), 8191)], no cutoff.             */
+/* inv_eps == NULL selects the constant dielectric (w already holds 332/diel).*/
+/* `out` receives nx*ny*nz FP32 values.  Synchronous.                        */
+/* ------------------------------------------------------------------------ */
+int ag_emap(ag_ctx* ctx, const ag_grid* grid, int n_atoms, const double* xyzw, const double* inv_eps,
+            float* out);
+
+/* Precision modes of the e-map accumulation (for the precision study). */
+#define AG_EMAP_KAHAN 0      /* Kahan-compensated FP32 per atom tile, FP64 across tiles (default) */
+#define AG_EMAP_PLAIN 1      /* plain FP32 accumulation over all atoms */
+int ag_emap_mode(ag_ctx* ctx, const ag_grid* grid, int n_atoms, const double* xyzw, const double* inv_eps,
+                 int mode, float* out);
+
+/* ------------------------------------------------------------------------ */
+/* Affinity maps + desolvation map in one fused pass.                        */
+/* Replaces calculateGridmaps (CalculateGridmaps.h:30-31, body               */
+/* CalculateGridmaps.cpp:433-485).  out_maps receives n_maps*nx*ny*nz FP32   */
+/* values (map-major), out_dmap nx*ny*nz.  Covalent maps are left untouched. */
+/* ------------------------------------------------------------------------ */
+int ag_affinity(ag_ctx* ctx, const ag_grid* grid, const ag_receptor* rec, const ag_affinity_params* par,
+                float* out_maps, float* out_dmap);
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident form, for callers that keep inputs in HBM between calls:  */
+/* ag_upload stages a job into context-owned device memory, ag_compute runs  */
+/* the kernels on it (AG_WORK_* bits), ag_download copies the maps back.     */
+/* ------------------------------------------------------------------------ */
+#define AG_WORK_EMAP 1
+#define AG_WORK_AFFINITY 2
+#define AG_WORK_ALL 3
+int ag_upload(ag_ctx* ctx, const ag_grid* grid, const ag_receptor* rec, const ag_affinity_params* par,
+              const double* inv_eps);
+int ag_compute(ag_ctx* ctx, int work);
+/* Device pointer to the map set [n_maps atom maps][e-map][d-map], FP32. */
+float* ag_device_maps(ag_ctx* ctx);
+/* out: (n_maps + 2) * nx*ny*nz floats in the same order. */
+int ag_download(ag_ctx* ctx, float* out);
+
+/* ------------------------------------------------------------------------ */
+/* Whole jobs (the drop-in for programMain, main.cpp:115-254).               */
+/* ------------------------------------------------------------------------ */
+typedef struct ag_problem_info {
+  int nx, ny, nz;
+  double spacing;
+  double center[3];
+  int n_atoms;
+  int n_maps;                  /* ligand maps; the set also has the e-map and d-map */
+  int n_types;
+  int dist_dep_diel;
+  int has_floating_grid;
+} ag_problem_info;
+
+/* Parse a GPF (and the PDBQT / parameter file it names) and precompute the
+ * tables and bond vectors, as InputDataLoader::load + main.cpp:163-193 do.
+ * Writes the .xyz file (on the GPF's gridcenter line) and the .fld file. */
+int ag_problem_load(const char* gpf_path, int use_v4_params, const char* log_path, ag_problem** out);
+void ag_problem_free(ag_problem* p);
+int ag_problem_info_get(const ag_problem* p, ag_problem_info* info);
+/* Views of the host arrays the GPU consumes (valid while p lives). */
+int ag_problem_views(const ag_problem* p, ag_grid* grid, ag_receptor* rec, ag_affinity_params* par,
+                     const double** inv_eps);
+/* Compute the whole map set on the GPU (also covalent maps and the floating grid). */
+int ag_problem_compute(ag_ctx* ctx, ag_problem* p);
+/* Host copy of the map set [n_maps][e][d], FP32 unrounded; n*(n_maps+2) floats. */
+const float* ag_problem_maps(const ag_problem* p);
+/* Write every .map file (and the floating grid) like GridMapList::saveGridMap. */
+int ag_problem_write(ag_problem* p);
+
+/* The autogrid4 / fastgrid4 command line (ProgramParameters.cpp:63-112). */
+int ag_main(int argc, char** argv);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic receptors for tests and benchmarks: a self-avoiding      */
+/* chain walk inside a sphere or ellipsoid, AutoDock4 types by fraction,     */
+/* charges N(0, sigma) clipped and shifted to a net charge, 3-decimal values.*/
+/* Writes <dir>/<stem>.pdbqt and <dir>/<stem>.gpf.                           */
+/* ------------------------------------------------------------------------ */
+typedef struct ag_synth_params {
+  uint64_t seed;
+  int n_atoms;
+  double semi_axes[3];         /* ellipsoid semi-axes in A (equal: sphere) */
+  double origin[3];            /* shape centre */
+  double frac_C, frac_OA, frac_N, frac_HD, frac_A, frac_SA;
+  double charge_sigma, charge_clip, net_charge;
+  int npts;                    /* GPF npts (even): npts+1 points per axis */
+  double spacing;
+  const char* ligand_types;    /* space-separated, e.g. "A C HD N OA SA" */
+  double dielectric;           /* GPF dielectric line value, e.g. -0.1465 */
+} ag_synth_params;
+int ag_synth_write(const char* dir, const char* stem, const ag_synth_params* sp);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FASTGRID_B200_H */
