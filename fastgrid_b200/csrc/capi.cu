@@ -562,6 +562,7 @@ extern "C" int ag_problem_load(const char* gpf, int v4, const char* log_path, ag
     P->lib.reset(new ag::ParamLib(v4 != 0));
     ag::loadGPF(P->p, *P->lib, P->log, gpf);
     ag::precompute(P->p, *P->lib, P->log);
+    ag::writeFld(P->p, P->log.programName.c_str(), P->log);
   } catch (ag::ExitProgram& e) {
     delete P;
     return fail(AG_E_HOST, "exit %d: %s", e.code, e.msg.c_str());

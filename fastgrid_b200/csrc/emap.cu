@@ -117,7 +117,15 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
       tma_load_1d(S.ring[slot ^ 1], P.atoms + t1, n1 * 32u, &S.bar[slot ^ 1]);
     }
     bool ok = mbar_wait_bounded(&S.bar[slot], (unsigned)(t >> 1) & 1u, P.status);
-    if (__syncthreads_or(!ok)) return;
+    if (__syncthreads_or(!ok)) {
+      // Give the copies still in flight (this tile's and the prefetched next
+      // one) a bounded chance to land before shared memory is released.
+      if (tid == 0) {
+        mbar_wait_bounded(&S.bar[slot], (unsigned)(t >> 1) & 1u, P.status);
+        if (t + 1 < ntiles) mbar_wait_bounded(&S.bar[slot ^ 1], (unsigned)((t + 1) >> 1) & 1u, P.status);
+      }
+      return;
+    }
 
     // Classify and convert this tile's atoms (one atom per thread).
     bool isNear = false;
