@@ -1,0 +1,306 @@
+#!/usr/bin/env python3
+"""Benchmark: one AutoGrid map set (e-map + 10 affinity maps + d-map) for the
+large synthetic configuration — 20,000 receptor atoms in a 45 x 35 x 30 A
+ellipsoid, 161^3 grid at 0.375 A, ligand types A C HD N NA OA SA S F Cl — on
+the B200 engine.
+
+A step is one map set.  `value` is point-atom evaluations per second over all
+ranks (N_atoms x N_points per map set / map-set seconds), with the inputs
+resident in HBM; `e2e` is the same metric through the public C ABI with host
+buffers (upload, compute, download of all maps).  L2 is flushed (256 MiB
+write) between timed steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times FastGrid's own CPU path (oracle/_ref/fastgrid4, built
+from the reference sources, all host threads) on a bounded sample of the same
+workload (a 161 x 161 x 21 slab of the grid) and reports the same metric.
+Under torchrun (N > 1) every rank computes its own map set on its own GPU
+(replicas; weak scaling); there is no inter-GPU exchange in this path.
+"""
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "map-set sec & point-atom evals/s, direct vs surrogate at stated error"
+UNIT = "point-atom evals/s"
+WORKLOAD = dict(n_atoms=20000, semi_axes=(45, 35, 30), npts=160, seed=2,
+                ligand_types="A C HD N NA OA SA S F Cl")
+SLAB_Z = 20          # CPU sample: npts 160 160 20 (161 x 161 x 21 points)
+REF_BIN = os.path.join(HERE, "oracle", "_ref", "fastgrid4")
+
+
+def config_dict(n_gpus, extra=None):
+    d = {"workload": "synthetic receptor 20000 atoms (45x35x30 A ellipsoid), 161^3 grid @0.375 A, "
+                     "10 ligand maps + e-map + d-map, distance-dependent dielectric",
+         "n_atoms": WORKLOAD["n_atoms"], "grid": [161, 161, 161], "ligand_types": WORKLOAD["ligand_types"],
+         "parallelism": f"replicas x{n_gpus}", "l2": "flushed between steps (256 MiB write)"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+def make_workload(d, npts_z=None):
+    import fastgrid_b200 as fg
+    gpf = fg.synth_write(d, "bench", **WORKLOAD)
+    if npts_z is not None:
+        txt = open(gpf).read()
+        txt = re.sub(r"^npts .*$", f"npts 160 160 {npts_z}", txt, flags=re.M)
+        open(gpf, "w").write(txt)
+    return gpf
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            self.p.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.p:
+            return None
+        rows = [l.split(",") for l in open(self.path).read().splitlines() if l.strip()]
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip() == "Active":
+                    reasons.add(n)
+        mx = [float(r[2]) for r in rows if len(r) > 2 and r[2].strip().replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def fastgrid_cpu_run(workdir, gpf):
+    """Run FastGrid's CPU build on `gpf`; return (map-set seconds, stderr)."""
+    r = subprocess.run([REF_BIN, "-p", os.path.basename(gpf), "-l", "ref.glg", "--benchmark"], cwd=workdir,
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("fastgrid4 (reference CPU) failed: " + r.stderr[-500:])
+    ms = 0.0
+    for phase in ("Cutoff grid", "KD-tree of hydrogens", "Atom & desolvation maps", "Electrostatic map"):
+        m = re.search(re.escape(phase) + r"\s+Real:\s+(\d+) ms", r.stderr)
+        if m:
+            ms += float(m.group(1))
+    return ms / 1e3, r.stderr
+
+
+def cpu_sample(tmp):
+    """FastGrid CPU on the 161 x 161 x 21 slab: (pairs/s, seconds, pairs)."""
+    d = os.path.join(tmp, "cpu_sample")
+    os.makedirs(d, exist_ok=True)
+    gpf = make_workload(d, npts_z=SLAB_Z)
+    secs, _ = fastgrid_cpu_run(d, gpf)
+    pairs = WORKLOAD["n_atoms"] * 161 * 161 * (SLAB_Z + 1)
+    return pairs / secs, secs, pairs
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    if not os.path.exists(REF_BIN):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fastgrid4 was not built "
+                          "(build() compiles it from the reference sources when they are present)"}))
+        return
+    with tempfile.TemporaryDirectory() as tmp:
+        d = os.path.join(tmp, "ref")
+        os.makedirs(d)
+        gpf = make_workload(d, npts_z=SLAB_Z)
+        pairs = WORKLOAD["n_atoms"] * 161 * 161 * (SLAB_Z + 1)
+        for _ in range(args.warmup):
+            fastgrid_cpu_run(d, gpf)
+        times = [fastgrid_cpu_run(d, gpf)[0] for _ in range(args.steps)]
+    secs = sum(times) / len(times)
+    value = pairs / secs
+    cores = os.cpu_count()
+    sample = (f"161x161x21 z-slab of the 161^3 grid (all 20000 atoms, {pairs:.3g} point-atom pairs) per step; "
+              "map-set time = FastGrid's own e-map + cutoff-grid + kd-tree + affinity phase times")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args.gpus, {"sample": sample}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "map_set_sec_sample": secs}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import numpy as np
+    import torch
+    import fastgrid_b200 as fg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    tmp = tempfile.mkdtemp()
+    try:
+        gpf = make_workload(tmp)
+        old = os.getcwd()
+        os.chdir(tmp)
+        prob = fg.Problem(os.path.basename(gpf), log="bench.glg")
+        os.chdir(old)
+        n_atoms, npts, nmaps = prob.info.n_atoms, prob.npoints, prob.n_maps
+        pairs = n_atoms * npts
+
+        rsqrt_ps, ffma_ps = fg.measure_peaks(local)
+        ctx = fg.Context(local)
+        stream = torch.cuda.ExternalStream(ctx.stream)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+        # ---- device-resident timing (value) ----
+        ctx.upload(prob.grid, prob.receptor, prob.params, prob.inv_eps_ptr)
+        for _ in range(args.warmup):
+            ctx.compute(fg.AG_WORK_ALL)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e_starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        e_ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        launches0 = ctx.launches
+        with ClockSampler(local) as clocks:
+            for k in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(k & 0xFF)
+                    starts[k].record(stream)
+                    e_starts[k].record(stream)
+                    ctx.compute(fg.AG_WORK_EMAP)
+                    e_ends[k].record(stream)
+                    ctx.compute(fg.AG_WORK_AFFINITY)
+                    ends[k].record(stream)
+            torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+        emap_ms = [s.elapsed_time(e) for s, e in zip(e_starts, e_ends)]
+        tot_ms = sum(step_ms)
+        if dist:
+            t = torch.tensor([tot_ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            tot_ms = float(t.item())
+        ms_step = tot_ms / args.steps
+        value = world * pairs / (ms_step * 1e-3)
+        emap_avg = sum(emap_ms) / len(emap_ms)
+        aff_avg = ms_step - emap_avg
+
+        # ---- end to end through the C ABI with host buffers ----
+        out = torch.empty((nmaps + 2) * npts, dtype=torch.float32, pin_memory=True)
+        outp = out.numpy()
+        h2d = n_atoms * (32 + 4 + 4 + 4 + 4 + 48) + 8192 * 4
+        h2d += prob.info.n_types * 801 * nmaps * 4
+        d2h = (nmaps + 2) * npts * 4
+        for _ in range(2):
+            ctx.upload(prob.grid, prob.receptor, prob.params, prob.inv_eps_ptr)
+            ctx.compute(fg.AG_WORK_ALL)
+            ctx.download(outp)
+        if dist:
+            dist.barrier()
+        e2e_t = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ctx.upload(prob.grid, prob.receptor, prob.params, prob.inv_eps_ptr)
+            ctx.compute(fg.AG_WORK_ALL)
+            ctx.download(outp)
+            e2e_t.append(time.perf_counter() - t0)
+        e2e_s = sum(e2e_t) / len(e2e_t)
+        if dist:
+            t = torch.tensor([e2e_s], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e_value = world * pairs / e2e_s
+        check = float(np.abs(outp[nmaps * npts:(nmaps + 1) * npts]).max())
+
+        # ---- CPU baseline (rank 0, N=1 only) ----
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
+            v, secs, sp = cpu_sample(tmp)
+            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"FastGrid CPU (oracle/_ref/fastgrid4, OpenMP) on the 161x161x21 z-slab, {sp:.3g} "
+                             f"pairs in {secs:.2f} s of e-map + affinity phases"}
+
+        emap_pairs_per_s = pairs / (emap_avg * 1e-3)
+        ck = clocks.summary()
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 (FP64 tile sums and exact FP64 bins near edges)",
+                "data": "synthetic", "config": config_dict(world),
+                "map_set_sec": ms_step * 1e-3, "emap_ms": emap_avg, "affinity_ms": aff_avg,
+                "roofline": {"bound": "sfu", "kernel": "emap_kernel",
+                             "achieved": emap_pairs_per_s / 1e9, "peak": rsqrt_ps / 1e9, "unit": "Gpair/s",
+                             "frac": emap_pairs_per_s / rsqrt_ps, "traffic": None,
+                             "note": "one SFU rsqrt per point-atom pair; peak = rsqrt/s measured by "
+                                     "ag_measure_peaks in this run (MEASURED_PEAKS.json has no SFU figure)"},
+                "roofline_fp32": {"achieved_ops": 8 * emap_pairs_per_s / 1e12, "peak": ffma_ps / 1e12,
+                                  "unit": "Tinstr/s", "frac": 8 * emap_pairs_per_s / ffma_ps,
+                                  "note": "8 algorithmic FP32-pipe ops per pair vs measured FFMA issue rate"},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": e2e_s * 1e3},
+                "gpu_launches": launches, "clocks": ck, "cpu_baseline": cpu,
+                "emap_abs_max": check,
+            }
+            print(json.dumps(line))
+        ctx.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -70,7 +70,7 @@ class SynthParams(C.Structure):
 EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", "ag_ctx_launch_count",
            "ag_emap", "ag_emap_mode", "ag_affinity", "ag_upload", "ag_compute", "ag_device_maps", "ag_download",
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
-           "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write"]
+           "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks"]
 
 _lib = None
 
@@ -113,6 +113,7 @@ def lib():
     L.ag_problem_write.argtypes = [vp]
     L.ag_main.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
     L.ag_synth_write.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(SynthParams)]
+    L.ag_measure_peaks.argtypes = [C.c_int, dp, dp]
     _lib = L
     return L
 
@@ -241,6 +242,13 @@ class Problem:
 
     def write(self):
         _check(lib().ag_problem_write(self.h))
+
+
+def measure_peaks(device=0):
+    """(SFU rsqrt/s, FP32 FMA instructions/s) measured on `device` now."""
+    a, b = C.c_double(), C.c_double()
+    _check(lib().ag_measure_peaks(device, C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def main(argv):

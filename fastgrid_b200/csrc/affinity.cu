@@ -1,26 +1,35 @@
 // Affinity maps for every ligand type plus the desolvation map, in one fused
 // pass over a device-built cell list (FastGrid CalculateGridmaps.cpp:84-316).
 //
-// For each grid point and each receptor atom within 8 A:
-//   r, unit vector, bin int(100 r)   (exactly as the reference: FP64, IEEE
-//                                     sqrt and reciprocal, no fused ops)
-//   directional H-bond factors racc / rdon / Hramp (FP64; :84-197)
-//   per map: E = table[type][bin][map], H-bond weighting or min/max
-//            bookkeeping, desolvation                (FP32; :199-236)
-//   d-map += solparQ * vol * sol[bin]                (FP32; :302)
-// then per map the H-bond min + max are added (:307-313).
+// For each grid point and each receptor atom within 8 A (:263-303):
+//   r, unit vector, bin = int(100 r)
+//   directional H-bond factors racc / rdon / Hramp            (:84-197)
+//   per map: E = table[type][bin][map] with the H-bond weighting or the
+//            min/max bookkeeping                              (:199-232)
+//   desolvation                                               (:234-235, :302)
+// then per map the H-bond min + max are added                 (:307-313).
 //
-// The nearest H donor of each point (the reference's kd-tree query,
-// :246-250) is found by a separate kernel over a donor-only cell list: it only
-// matters for a donor atom within 8 A, so searching the cells that cover the
-// 8 A sphere is exact.
+// Arithmetic.  Geometry is FP32 in a CTA-local frame (atoms and points within
+// ~12 A of the frame origin, so coordinates keep ~1e-6 A).  The three places
+// where the reference's FP64 result is a step function of the geometry are
+// decided exactly: the 8 A cutoff, the 0.01 A table bin and the sign of
+// cos(theta) for D1 and ordered A2 atoms.  When the FP32 value lies within a
+// guard band of such an edge, that decision is recomputed in FP64 exactly as
+// the reference computes it (same operations, no fused multiply-adds; the bin
+// through a table of r^2 thresholds).  Everything else is continuous in the
+// geometry and stays FP32.
 //
-// Schedule: one CTA per 8x8x4 block of points, one point per thread.  The CTA
-// gathers the atoms of the 8 A cells around its box that lie within 8 A of
-// the box into shared memory (batches of kCap), and every thread walks that
-// list.  The pair-energy tables for the maps of this pass sit in shared memory
-// as FP32 (rows for r <= 8 A only); maps are split into passes so that
-// ntypes * 801 * G floats fit.
+// The desolvation terms are linear in two per-point sums,
+//   S1 = sum sol(r) vol_a,  S2 = sum sol(r) (solpar_a + solparQ |q_a|),
+// so map m receives solparProbe_m S1 + volProbe_m S2 and the d-map solparQ S1.
+//
+// Schedule.  One CTA per 8x8x4 block of points, one point per thread.  The
+// CTA gathers the atoms of the 8 A cells around its box that lie within 8 A of
+// the box (shared memory, batches of kCap), orders them by receptor type, and
+// walks one type at a time with that type's FP32 table rows (801 x nmPad) in
+// shared memory, fetched by TMA bulk copies into two buffers so the next
+// type's rows load while the current type is processed.  All branches on the
+// atom's H-bond class and the map's H-bond mode are uniform across the CTA.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -33,93 +42,61 @@ namespace agk {
 using namespace agd;
 
 constexpr int kAffThreads = kAffTX * kAffTY * kAffTZ;  // 256
-constexpr int kCap = 256;                              // candidate atoms per batch
+constexpr int kCap = 384;                              // candidate atoms per batch
 enum { NON = 0, DS = 1, D1 = 2, AS = 3, A1 = 4, A2 = 5 };
 #define AG_PI 3.14159265358979323846
 
-struct Cand {
-  double x, y, z;
-  double rv[3], rv2[3];
-  int info, idx;
+struct CandF {          // FP32 view, CTA-local coordinates
+  float x, y, z;
+  int idx;
   float vol, solq;
+  int info;
+  float pad;
+  float rv[3], rv2[3];  // unit vectors
 };
 
-struct AffSmemHead {
-  Cand cand[kCap];
-  float sol[kAffRows + 3];
+struct AffSmem {
+  CandF cand[kCap];
+  double cx[kCap], cy[kCap], cz[kCap];  // FP64 grid-centred coordinates (exact fallbacks)
+  short perm[kCap];
+  int typeStart[kMaxTypes + 1];
+  int run[kMaxTypes + 1];
   int cnt[kAffThreads / 32];
+  float sol[kAffRows + 3];
+  uint64_t bar[2];
 };
 
-size_t aff_smem_bytes(int ntypes, int G) {
-  return sizeof(AffSmemHead) + sizeof(float) * (size_t)(ntypes + 1) * kAffRows * G;
+size_t aff_smem_bytes(int nmPad) {
+  return ((sizeof(AffSmem) + 127) / 128) * 128 + 2 * sizeof(float) * (size_t)kAffRows * nmPad;
 }
 
-__device__ __forceinline__ double dot3(const double* a, double x, double y, double z) {
-  return __dadd_rn(__dadd_rn(__dmul_rn(x, a[0]), __dmul_rn(y, a[1])), __dmul_rn(z, a[2]));
-}
-__device__ __forceinline__ double acos_c(double f) { return (f > 1) ? 0.0 : (f < -1) ? AG_PI : acos(f); }
+__device__ __forceinline__ float acosf_c(float f) { return (f > 1.f) ? 0.f : (f < -1.f) ? 3.14159265f : acosf(f); }
 
-// Directional H-bond factors (CalculateGridmaps.cpp:84-197), FP64.
-__device__ void hbond_angular(const Cand& a, int hb, const double* rvClosest, bool isClosest, double ux, double uy,
-                              double uz, double& racc, double& rdon, double& Hramp) {
-  racc = 1; rdon = 1; Hramp = 1;
-  const double cosTheta = -dot3(a.rv, ux, uy, uz);
-  if (hb == D1) {
-    racc = 0;
-    if (cosTheta > 0) {
-      double ra = cosTheta;
-      const int rexp = (a.info >> 9) & 7;
-      if (rexp == 4) ra = ra * ra;
-      if (rexp == 4 || rexp == 2) ra = ra * ra;
-      racc = ra;
-      if (!isClosest && rvClosest) {
-        const double c = __dadd_rn(__dadd_rn(__dmul_rn(rvClosest[0], a.rv[0]), __dmul_rn(rvClosest[1], a.rv[1])),
-                                   __dmul_rn(rvClosest[2], a.rv[2]));
-        const double theta = acos_c(c);
-        Hramp = 0.5 - 0.5 * cos(theta * (120.0 / 90.0));
-      }
-    }
-  } else if (hb == A1) {
-    rdon = 0;
-    if (cosTheta > 0) rdon = cosTheta * cosTheta;
-  } else if (hb == A2) {
-    rdon = 0;
-    if ((a.info >> 8) & 1) {
-      racc = 0;
-      const double theta = acos_c(cosTheta);
-      if (theta <= 1.24791 + (AG_PI / 2)) {
-        const double c = cos(theta - 1.24791);
-        rdon = (c * c) * (c * c);
-        racc = rdon;
-      }
-    } else {
-      double rd = 0;
-      if (cosTheta >= 0) {
-        // cross(u, rvector2)
-        const double cx = __dsub_rn(__dmul_rn(uy, a.rv2[2]), __dmul_rn(uz, a.rv2[1]));
-        const double cy = __dsub_rn(__dmul_rn(uz, a.rv2[0]), __dmul_rn(ux, a.rv2[2]));
-        const double cz = __dsub_rn(__dmul_rn(ux, a.rv2[1]), __dmul_rn(uy, a.rv2[0]));
-        double rd2 = __dadd_rn(__dadd_rn(__dmul_rn(cx, cx), __dmul_rn(cy, cy)), __dmul_rn(cz, cz));
-        if (rd2 < 1.0e-6) rd2 = 1.0e-6;
-        const double inv_rd = __drcp_rn(__dsqrt_rn(rd2));
-        const double ti = fabs(acos_c(__dmul_rn(inv_rd, dot3(a.rv, cx, cy, cz))) - (AG_PI / 2));
-        rd = 0.9 + 0.1 * sin(ti + ti);
-      } else if (cosTheta >= -0.34202) {
-        const double q = 0.116978 - cosTheta * cosTheta;
-        rd = 562.25 * (q * q * q);
-      }
-      const double t0 = (AG_PI / 2) - acos_c(dot3(a.rv2, ux, uy, uz));
-      rdon = rd * cos(t0);
-    }
-  }
+// Exact FP64 squared distance as the reference forms it (Vec3d::MagnitudeSqr
+// of atom - gridPos, left to right, separately rounded).
+__device__ __forceinline__ double rsq_exact(double ax, double ay, double az, double gx, double gy, double gz) {
+  const double dx = __dsub_rn(ax, gx), dy = __dsub_rn(ay, gy), dz = __dsub_rn(az, gz);
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
 
+// Exact FP64 cos(theta) = -dot(unit(atom - gridPos), rvector) (CalculateGridmaps.cpp:89).
+__device__ double costheta_exact(double ax, double ay, double az, double gx, double gy, double gz, const double* rv) {
+  const double dx = __dsub_rn(ax, gx), dy = __dsub_rn(ay, gy), dz = __dsub_rn(az, gz);
+  double rSq = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  if (rSq < 1.0e-24) rSq = 1.0e-24;
+  const double invR = __drcp_rn(__dsqrt_rn(rSq));
+  const double ux = __dmul_rn(dx, invR), uy = __dmul_rn(dy, invR), uz = __dmul_rn(dz, invR);
+  return -__dadd_rn(__dadd_rn(__dmul_rn(ux, rv[0]), __dmul_rn(uy, rv[1])), __dmul_rn(uz, rv[2]));
+}
+
+template <int NMAX>
 __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  AffSmemHead& S = *reinterpret_cast<AffSmemHead*>(smem_raw);
-  float* tab = reinterpret_cast<float*>(smem_raw + sizeof(AffSmemHead));
-  float* tabH = tab + (size_t)P.ntypes * kAffRows * P.G;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  AffSmem& S = *reinterpret_cast<AffSmem*>(smem_raw);
+  float* tabBuf = reinterpret_cast<float*>(smem_raw + ((sizeof(AffSmem) + 127) / 128) * 128);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nmPad = P.nmPad;
+  const unsigned tabBytes = (unsigned)(kAffRows * nmPad * sizeof(float));
 
   // This CTA's block of points and this thread's point.
   const int tbx = (P.nx + kAffTX - 1) / kAffTX, tby = (P.ny + kAffTY - 1) / kAffTY;
@@ -128,47 +105,52 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
   const int ix = x0 + (tid % kAffTX), iy = y0 + (tid / kAffTX) % kAffTY, iz = z0 + tid / (kAffTX * kAffTY);
   const bool valid = ix < P.nx && iy < P.ny && iz < P.nz;
   const double h = P.h;
+  // FP64 point as the reference forms it, and FP32 point in the CTA frame
+  // (origin on the lattice point (x0, y0, z0): local coordinates are exact).
   const double gx = __dmul_rn((double)(ix - P.n2x), h), gy = __dmul_rn((double)(iy - P.n2y), h),
                gz = __dmul_rn((double)(iz - P.n2z), h);
+  const double ox = __dmul_rn((double)(x0 - P.n2x), h), oy = __dmul_rn((double)(y0 - P.n2y), h),
+               oz = __dmul_rn((double)(z0 - P.n2z), h);
+  const float px = (float)(gx - ox), py = (float)(gy - oy), pz = (float)(gz - oz);
   const int64_t pt = ((int64_t)iz * P.ny + iy) * P.nx + ix;
 
   double lo[3], hi[3];
-  lo[0] = (double)(x0 - P.n2x) * h; hi[0] = (double)(min(x0 + kAffTX, P.nx) - 1 - P.n2x) * h;
-  lo[1] = (double)(y0 - P.n2y) * h; hi[1] = (double)(min(y0 + kAffTY, P.ny) - 1 - P.n2y) * h;
-  lo[2] = (double)(z0 - P.n2z) * h; hi[2] = (double)(min(z0 + kAffTZ, P.nz) - 1 - P.n2z) * h;
+  lo[0] = ox; hi[0] = (double)(min(x0 + kAffTX, P.nx) - 1 - P.n2x) * h;
+  lo[1] = oy; hi[1] = (double)(min(y0 + kAffTY, P.ny) - 1 - P.n2y) * h;
+  lo[2] = oz; hi[2] = (double)(min(z0 + kAffTZ, P.nz) - 1 - P.n2z) * h;
   int c0[3], c1[3];
   for (int d = 0; d < 3; d++) {
     c0[d] = max(0, (int)floor((lo[d] - 8.0 - P.cellLo[d]) / 8.0));
     c1[d] = min(P.ncell[d] - 1, (int)floor((hi[d] + 8.0 - P.cellLo[d]) / 8.0));
   }
 
-  // Tables of this pass -> shared memory.
-  {
-    const int n = P.ntypes * kAffRows * P.G;
-    for (int i = tid; i < n; i += kAffThreads) tab[i] = P.table[i];
-    if (P.tableH)
-      for (int i = tid; i < kAffRows * P.G; i += kAffThreads) tabH[i] = P.tableH[i];
-    for (int i = tid; i < kAffRows; i += kAffThreads) S.sol[i] = P.sol[i];
+  for (int i = tid; i < kAffRows; i += kAffThreads) S.sol[i] = P.sol[i];
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_barrier_init();
   }
 
   const int ch = valid ? P.closestH[pt] : -1;
-  double rvC[3] = {0, 0, 0};
-  if (ch >= 0) { rvC[0] = P.rv[3 * ch]; rvC[1] = P.rv[3 * ch + 1]; rvC[2] = P.rv[3 * ch + 2]; }
+  float rcx = 0.f, rcy = 0.f, rcz = 0.f;
+  if (ch >= 0) { rcx = P.rv[3 * ch]; rcy = P.rv[3 * ch + 1]; rcz = P.rv[3 * ch + 2]; }
 
-  float em[kAffMaxGroup], mn[kAffMaxGroup], mx[kAffMaxGroup];
-  unsigned hbFlag = 0;
+  float em[NMAX], mn[kMaxMinMax], mx[kMaxMinMax];
 #pragma unroll
-  for (int g = 0; g < kAffMaxGroup; g++) { em[g] = 0.f; mn[g] = 999999.f; mx[g] = -999999.f; }
-  float ed = 0.f;
+  for (int g = 0; g < NMAX; g++) em[g] = 0.f;
+#pragma unroll
+  for (int s = 0; s < kMaxMinMax; s++) { mn[s] = 999999.f; mx[s] = -999999.f; }
+  unsigned mmFlag = 0;
+  float S1 = 0.f, S2 = 0.f;
 
-  // Iterate over the cells around the box in fixed order; gather batches.
   const int ncx = c1[0] - c0[0] + 1, ncy = c1[1] - c0[1] + 1, ncz = c1[2] - c0[2] + 1;
   const int ncells = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy * ncz : 0;
   int ci = 0, pos = 0;
+  unsigned phaseBits = 0u;
   __syncthreads();
   while (ci < ncells) {
+    // ---- gather one batch of candidates (file order within cells) ----
     int nb = 0;
-    // Fill one batch.
     while (ci < ncells) {
       const int cx = c0[0] + ci % ncx, cy = c0[1] + (ci / ncx) % ncy, cz = c0[2] + ci / (ncx * ncy);
       const int cell = (cz * P.ncell[1] + cy) * P.ncell[0] + cx;
@@ -178,13 +160,14 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
       if (nb + cnt > kCap) break;
       bool keep = false;
       int atom = -1;
+      double4 a = make_double4(0, 0, 0, 0);
       if (tid < cnt) {
         atom = P.cellAtoms[cbeg + pos + tid];
-        const double4 a = P.xyz[atom];
+        a = P.xyz[atom];
         const double ddx = fmax(fmax(lo[0] - a.x, a.x - hi[0]), 0.0);
         const double ddy = fmax(fmax(lo[1] - a.y, a.y - hi[1]), 0.0);
         const double ddz = fmax(fmax(lo[2] - a.z, a.z - hi[2]), 0.0);
-        keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.000001;
+        keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.001;
       }
       const unsigned kb = __ballot_sync(0xffffffffu, keep);
       if (lane == 0) S.cnt[warp] = __popc(kb);
@@ -196,14 +179,16 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
         total += S.cnt[w];
       }
       if (keep) {
-        Cand& c = S.cand[nb + off + __popc(kb & ((1u << lane) - 1u))];
-        const double4 a = P.xyz[atom];
-        c.x = a.x; c.y = a.y; c.z = a.z;
-        for (int k = 0; k < 3; k++) { c.rv[k] = P.rv[3 * atom + k]; c.rv2[k] = P.rv2[3 * atom + k]; }
-        c.info = P.info[atom];
+        const int j = nb + off + __popc(kb & ((1u << lane) - 1u));
+        CandF& c = S.cand[j];
+        c.x = (float)(a.x - ox); c.y = (float)(a.y - oy); c.z = (float)(a.z - oz);
         c.idx = atom;
         c.vol = P.vol[atom];
         c.solq = P.solq[atom];
+        c.info = P.info[atom];
+        c.rv[0] = P.rv[3 * atom]; c.rv[1] = P.rv[3 * atom + 1]; c.rv[2] = P.rv[3 * atom + 2];
+        c.rv2[0] = P.rv2[3 * atom]; c.rv2[1] = P.rv2[3 * atom + 1]; c.rv2[2] = P.rv2[3 * atom + 2];
+        S.cx[j] = a.x; S.cy[j] = a.y; S.cz[j] = a.z;
       }
       nb += total;
       pos += cnt;
@@ -211,77 +196,228 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
       __syncthreads();
     }
 
-    // Walk the batch.
-    if (valid) {
-      for (int j = 0; j < nb; j++) {
-        const Cand& a = S.cand[j];
-        double dx = a.x - gx, dy = a.y - gy, dz = a.z - gz;
-        double rSq = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-        if (rSq > 64.0) continue;
-        const int t = a.info & 31, hb = (a.info >> 5) & 7, dis = (a.info >> 8) & 1;
-        if (t == P.hydrogen && dis) continue;
-        if (rSq < 1.0e-24) rSq = 1.0e-24;
-        const double invR = __drcp_rn(__dsqrt_rn(rSq));
-        dx = __dmul_rn(dx, invR); dy = __dmul_rn(dy, invR); dz = __dmul_rn(dz, invR);
-        int iR = (int)__dmul_rn(__drcp_rn(invR), 100.0);
-        iR = min(iR, kAffRows - 1);
-        double racc, rdon, Hramp;
-        hbond_angular(a, hb, ch >= 0 ? rvC : nullptr, a.idx == ch, dx, dy, dz, racc, rdon, Hramp);
-        const float fracc = (float)racc, frdon = (float)rdon, fH = (float)Hramp;
-        const float s = S.sol[iR];
-        const float* row = tab + ((size_t)t * kAffRows + iR) * P.G;
-        const bool donorAtom = (hb == DS || hb == D1);
-#pragma unroll
-        for (int g = 0; g < kAffMaxGroup; g++) {
-          if (g >= P.G) break;
-          if (P.mapCov[g]) continue;
-          const float pwi = row[g];
-          if (P.mapIsHB[g]) {
-            const float rsph = fminf(fmaxf(pwi * 0.01f, 0.f), 1.f);
-            const int mhb = P.mapHbond[g];
-            if ((mhb == AS || mhb == A2) && donorAtom) {
-              float e = pwi;
-              if (dis) e = P.tableH ? tabH[max(0, iR - 110) * P.G + g] : 0.f;
-              em[g] += e * fH * (fracc + (1.f - fracc) * rsph);
-            } else if (mhb == A1 && donorAtom) {
-              const float v = pwi * (fracc + (1.f - fracc) * rsph);
-              mn[g] = fminf(mn[g], v); mx[g] = fmaxf(mx[g], v); hbFlag |= 1u << g;
-            } else if ((mhb == DS || mhb == D1) && hb >= AS) {
-              const float v = pwi * (frdon + (1.f - frdon) * rsph);
-              mn[g] = fminf(mn[g], v); mx[g] = fmaxf(mx[g], v); hbFlag |= 1u << g;
-            } else {
-              em[g] += pwi;
-            }
-          } else {
-            em[g] += pwi;
-          }
-          em[g] += s * (P.solparProbe[g] * a.vol + a.solq * P.volProbe[g]);
+    // ---- order the batch by receptor type (stable counting sort, one warp) ----
+    if (warp == 0) {
+      for (int t = lane; t <= kMaxTypes; t += 32) S.run[t] = 0;
+      __syncwarp();
+      for (int base = 0; base < nb; base += 32) {
+        const int j = base + lane;
+        const int key = j < nb ? (S.cand[j].info & 31) : 64 + lane;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (j < nb && lane == __ffs(grp) - 1) S.run[key] += __popc(grp);
+        __syncwarp();
+      }
+      if (lane == 0) {
+        int s = 0;
+        for (int t = 0; t < P.ntypes; t++) {
+          S.typeStart[t] = s;
+          s += S.run[t];
+          S.run[t] = S.typeStart[t];
         }
-        ed += P.solparQ * a.vol * s;
+        S.typeStart[P.ntypes] = s;
+      }
+      __syncwarp();
+      for (int base = 0; base < nb; base += 32) {
+        const int j = base + lane;
+        const int key = j < nb ? (S.cand[j].info & 31) : 64 + lane;
+        const unsigned grp = __match_any_sync(0xffffffffu, key);
+        if (j < nb) S.perm[S.run[key] + __popc(grp & ((1u << lane) - 1u))] = (short)j;
+        __syncwarp();
+        if (j < nb && lane == __ffs(grp) - 1) S.run[key] += __popc(grp);
+        __syncwarp();
       }
     }
     __syncthreads();
+
+    // ---- walk the batch one receptor type at a time ----
+    int slot = 0;
+    int t = 0;
+    while (t < P.ntypes && S.typeStart[t + 1] == S.typeStart[t]) t++;
+    if (t < P.ntypes && tid == 0) {
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&S.bar[0], tabBytes);
+      tma_load_1d(tabBuf, P.table + (size_t)t * kAffRows * nmPad, tabBytes, &S.bar[0]);
+    }
+    while (t < P.ntypes) {
+      int tn = t + 1;
+      while (tn < P.ntypes && S.typeStart[tn + 1] == S.typeStart[tn]) tn++;
+      if (tn < P.ntypes && tid == 0) {
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&S.bar[slot ^ 1], tabBytes);
+        tma_load_1d(tabBuf + (size_t)(slot ^ 1) * kAffRows * nmPad, P.table + (size_t)tn * kAffRows * nmPad, tabBytes,
+                    &S.bar[slot ^ 1]);
+      }
+      // Phase bits of the two buffers' barriers, kept in one word (bit b = buffer b).
+      const bool ok = mbar_wait_bounded(&S.bar[slot], (phaseBits >> slot) & 1u, P.status);
+      phaseBits ^= 1u << slot;
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0 && tn < P.ntypes) mbar_wait_bounded(&S.bar[slot ^ 1], (phaseBits >> (slot ^ 1)) & 1u, P.status);
+        return;
+      }
+      const float* tab = tabBuf + (size_t)slot * kAffRows * nmPad;
+      const int hb = P.typeHbond[t];
+      const bool skipDisH = (t == P.hydrogen);
+      const unsigned modes = P.typeModes[t];       // 2 bits per map
+      const bool needAng = P.typeNeedsAngular[t];
+
+      if (valid) {
+        for (int jj = S.typeStart[t]; jj < S.typeStart[t + 1]; jj++) {
+          const int j = S.perm[jj];
+          const CandF& a = S.cand[j];
+          const float dx = a.x - px, dy = a.y - py, dz = a.z - pz;
+          float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+          if (r2 > 64.0002f) continue;
+          const int dis = (a.info >> 8) & 1;
+          if (skipDisH && dis) continue;
+          double rSq64 = -1.0;
+          if (r2 > 63.9998f) {
+            rSq64 = rsq_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz);
+            if (rSq64 > 64.0) continue;
+          }
+          r2 = fmaxf(r2, 1.0e-24f);
+          const float rs = rsqrt_approx(r2);
+          const float T = r2 * (rs * 100.f);
+          const float kr = (T + 12582912.f) - 12582912.f;
+          int iR = min((int)__fmaf_rd(r2, rs * 100.f, 0.f), kAffRows - 1);
+          if (fabsf(T - kr) < P.delta && kr >= 1.f && kr <= (float)(kAffRows - 1)) {
+            if (rSq64 < 0.0) rSq64 = rsq_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz);
+            const int k = (int)kr;
+            iR = (rSq64 >= P.thr[k]) ? k : k - 1;
+          }
+          const float ux = dx * rs, uy = dy * rs, uz = dz * rs;
+
+          // Directional factors (CalculateGridmaps.cpp:84-197).
+          float racc = 1.f, rdon = 1.f, Hramp = 1.f;
+          if (needAng) {
+            float cosT = -(ux * a.rv[0] + uy * a.rv[1] + uz * a.rv[2]);
+            bool gt0 = cosT > 0.f, ge0 = cosT >= 0.f;
+            if ((hb == D1 || (hb == A2 && !dis)) && fabsf(cosT) < 1.0e-5f) {
+              // The D1 and ordered-A2 factors jump where cos(theta) changes sign:
+              // take the sign from the reference's FP64 expression.
+              const double c64 = costheta_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz, P.rv64 + 3 * a.idx);
+              cosT = (float)c64;
+              gt0 = c64 > 0.0;
+              ge0 = c64 >= 0.0;
+            }
+            if (hb == D1) {
+              racc = 0.f;
+              if (gt0) {
+                float ra = cosT;
+                const int rexp = (a.info >> 9) & 7;
+                if (rexp == 4) ra = ra * ra;
+                if (rexp == 4 || rexp == 2) ra = ra * ra;
+                racc = ra;
+                if (a.idx != ch && ch >= 0) {
+                  const float c = rcx * a.rv[0] + rcy * a.rv[1] + rcz * a.rv[2];
+                  Hramp = 0.5f - 0.5f * cosf(acosf_c(c) * (120.f / 90.f));
+                }
+              }
+            } else if (hb == A1) {
+              rdon = gt0 ? cosT * cosT : 0.f;
+            } else if (hb == A2) {
+              if (dis) {
+                // theta <= 1.24791 + pi/2  <=>  cos(theta) >= -sin(1.24791)
+                racc = 0.f;
+                rdon = 0.f;
+                if (cosT >= -0.94832352f) {
+                  const float s = sqrtf(fmaxf(0.f, 1.f - cosT * cosT));
+                  const float c = cosT * 0.31730505f + s * 0.94832352f;  // cos(theta - 1.24791)
+                  rdon = (c * c) * (c * c);
+                  racc = rdon;
+                }
+              } else {
+                float rd = 0.f;
+                if (ge0) {
+                  // sin(2 ti) with ti = |acos(x) - pi/2| = |asin(x)|:  2 |x| sqrt(1 - x^2)
+                  const float cxp = uy * a.rv2[2] - uz * a.rv2[1];
+                  const float cyp = uz * a.rv2[0] - ux * a.rv2[2];
+                  const float czp = ux * a.rv2[1] - uy * a.rv2[0];
+                  const float rd2 = fmaxf(cxp * cxp + cyp * cyp + czp * czp, 1.0e-6f);
+                  float x = rsqrt_approx(rd2) * (cxp * a.rv[0] + cyp * a.rv[1] + czp * a.rv[2]);
+                  x = fminf(fabsf(x), 1.f);
+                  rd = 0.9f + 0.2f * x * sqrtf(fmaxf(0.f, 1.f - x * x));
+                } else if (cosT >= -0.34202f) {
+                  const float q = 0.116978f - cosT * cosT;
+                  rd = 562.25f * (q * q * q);
+                }
+                // cos(pi/2 - acos(y)) = sqrt(1 - y^2), y = dot(u, rvector2)
+                const float y = ux * a.rv2[0] + uy * a.rv2[1] + uz * a.rv2[2];
+                rdon = rd * sqrtf(fmaxf(0.f, 1.f - y * y));
+              }
+            }
+          }
+
+          const float sv = S.sol[iR];
+          S1 = fmaf(sv, a.vol, S1);
+          S2 = fmaf(sv, a.solq, S2);
+          const float* row = tab + iR * nmPad;
+          const float wAcc = Hramp, fAcc = racc, fDon = rdon;
+#pragma unroll
+          for (int g = 0; g < NMAX; g++) {
+            if (g >= P.nmaps) break;
+            const float pwi = row[g];
+            const unsigned mode = (modes >> (2 * g)) & 3u;
+            if (mode == 0u) {
+              em[g] += pwi;
+            } else {
+              const float rsph = fminf(fmaxf(pwi * 0.01f, 0.f), 1.f);
+              if (mode == 1u) {
+                const float e = dis ? (P.tableH ? P.tableH[max(0, iR - 110) * nmPad + g] : 0.f) : pwi;
+                em[g] += e * wAcc * (fAcc + (1.f - fAcc) * rsph);
+              } else {
+                const float f = (mode == 2u) ? fAcc : fDon;
+                const float v = pwi * (f + (1.f - f) * rsph);
+                const int slot = P.mapMinMaxSlot[g];
+#pragma unroll
+                for (int s = 0; s < kMaxMinMax; s++)
+                  if (s == slot) {
+                    mn[s] = fminf(mn[s], v);
+                    mx[s] = fmaxf(mx[s], v);
+                  }
+                mmFlag |= 1u << slot;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();  // this buffer is free for the type after next
+      slot ^= 1;
+      t = tn;
+    }
   }
 
   if (!valid) return;
 #pragma unroll
-  for (int g = 0; g < kAffMaxGroup; g++) {
-    if (g >= P.G) break;
+  for (int g = 0; g < NMAX; g++) {
+    if (g >= P.nmaps) break;
     if (P.mapCov[g]) continue;
-    float e = em[g];
-    if (hbFlag & (1u << g)) e += mn[g] + mx[g];
-    P.out[(int64_t)(P.m0 + g) * P.npoints + pt] = e;
+    float e = em[g] + (P.solparProbe[g] * S1 + P.volProbe[g] * S2);
+    const int slot = P.mapMinMaxSlot[g];
+#pragma unroll
+    for (int s = 0; s < kMaxMinMax; s++)
+      if (s == slot && (mmFlag & (1u << s))) e += mn[s] + mx[s];
+    P.out[(int64_t)g * P.npoints + pt] = e;
   }
-  if (P.doDmap) P.dmap[pt] = ed;
+  P.dmap[pt] = P.solparQ * S1;
 }
 
 cudaError_t aff_launch(const AffParams& P, cudaStream_t st) {
-  const size_t smem = aff_smem_bytes(P.ntypes, P.G);
-  cudaError_t e = cudaFuncSetAttribute(affinity_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
+  const size_t smem = aff_smem_bytes(P.nmPad);
   const int tbx = (P.nx + kAffTX - 1) / kAffTX, tby = (P.ny + kAffTY - 1) / kAffTY,
             tbz = (P.nz + kAffTZ - 1) / kAffTZ;
-  affinity_kernel<<<tbx * tby * tbz, kAffThreads, smem, st>>>(P);
+  const int grid = tbx * tby * tbz;
+  cudaError_t e;
+#define AG_AFF(N)                                                                                           \
+  do {                                                                                                      \
+    e = cudaFuncSetAttribute(affinity_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);  \
+    if (e != cudaSuccess) return e;                                                                         \
+    affinity_kernel<N><<<grid, kAffThreads, smem, st>>>(P);                                                 \
+  } while (0)
+  if (P.nmaps <= 4) AG_AFF(4);
+  else if (P.nmaps <= 8) AG_AFF(8);
+  else if (P.nmaps <= 12) AG_AFF(12);
+  else AG_AFF(16);
+#undef AG_AFF
   return cudaGetLastError();
 }
 
@@ -355,8 +491,7 @@ cudaError_t cells_launch(const CellBuild& C, int ncellTotal, cudaStream_t st) {
   cell_count_kernel<<<blocks, 256, 0, st>>>(C);
   cell_scan_kernel<<<1, 1024, 0, st>>>(C.count, ncellTotal, C.cellStart);
   cell_scatter_kernel<<<blocks, 256, 0, st>>>(C);
-  // `count` is free again: reuse it as the sort's scratch (it holds ncell+1 >= n entries only if
-  // ncell+1 >= n; use cellOf, which holds n_atoms entries, instead).
+  // cellOf (n_atoms entries) is free after the scatter and serves as the sort's scratch.
   cell_sort_kernel<<<max(1, min(2048, (ncellTotal + 7) / 8)), 256, 0, st>>>(C.cellStart, ncellTotal, C.cellAtoms,
                                                                          C.cellOf);
   return cudaGetLastError();
@@ -364,7 +499,8 @@ cudaError_t cells_launch(const CellBuild& C, int ncellTotal, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // Nearest H donor per grid point (argmin over DS/D1 atoms within the 27 cells
-// around the point's cell, ties to the lower file index).
+// around the point's cell, ties to the lower file index), FP64 like the
+// reference's kd-tree query (CalculateGridmaps.cpp:246-250).
 // ---------------------------------------------------------------------------
 __global__ void closest_h_kernel(ClosestHParams P) {
   for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.npoints;
@@ -385,8 +521,7 @@ __global__ void closest_h_kernel(ClosestHParams P) {
           for (int j = P.cellStart[c]; j < P.cellStart[c + 1]; j++) {
             const int ia = P.cellAtoms[j];
             const double4 a = P.xyz[ia];
-            const double ex = a.x - gx, ey = a.y - gy, ez = a.z - gz;
-            const double r = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+            const double r = rsq_exact(a.x, a.y, a.z, gx, gy, gz);
             if (r < bestR || (r == bestR && ia < best)) { bestR = r; best = ia; }
           }
         }

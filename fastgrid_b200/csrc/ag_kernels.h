@@ -16,7 +16,10 @@ constexpr int kEmapPlain = 1;
 struct EmapBlock {
   int item0, nitems;
   double ox, oy, oz;
-  float hx, hy, hz, pad;
+  float hx, hy, hz;
+  float rfar2;                    // (100 * rFar)^2, rFar >= 50 A
+  int clampMid;                   // 1 if rFar + box diagonal can reach 81.9 A: clamp mid-list bins at 8191
+  int pad;
 };
 
 struct EmapParams {
@@ -43,18 +46,25 @@ size_t emap_smem_bytes();
 // Affinity + desolvation
 // ---------------------------------------------------------------------------
 constexpr int kAffTX = 8, kAffTY = 8, kAffTZ = 4;   // points per CTA (one per thread)
-constexpr int kAffMaxGroup = 8;                     // maps per pass
 constexpr int kAffRows = 801;                       // table rows kept: r <= 8 A
+constexpr int kMaxTypes = 32;                       // receptor types
+constexpr int kMaxMapsPass = 16;                    // ligand maps per pass
+constexpr int kMaxMinMax = 4;                       // maps per pass with H-bond min/max bookkeeping
 
+// Per (receptor type, map) H-bond handling, 2 bits per map in typeModes[t]
+// (CalculateGridmaps.cpp:206-228): 0 add E; 1 acceptor probe vs donor atom
+// (Hramp, racc weighting); 2 A1 probe vs donor atom (min/max, racc);
+// 3 donor probe vs acceptor atom (min/max, rdon).
 struct AffParams {
   // receptor (device)
   int n_atoms;
-  const double4* xyz;             // x, y, z, unused
+  const double4* xyz;             // FP64 grid-centred x, y, z (w unused)
   const int* info;                // type | hbond << 5 | disorder << 8 | rexp << 9
   const float* vol;
   const float* solq;              // solpar + solparQ * |q|
-  const double* rv;               // rvector, 3 per atom
-  const double* rv2;              // rvector2, 3 per atom
+  const float* rv;                // rvector, 3 per atom (FP32)
+  const float* rv2;               // rvector2, 3 per atom (FP32)
+  const double* rv64;             // rvector, 3 per atom (FP64, for exact sign decisions)
   // cell list (8 A cells)
   const int* cellStart;           // ncell + 1
   const int* cellAtoms;
@@ -66,19 +76,25 @@ struct AffParams {
   int64_t npoints;
   double h;
   // maps of this pass
-  int m0, G, nmaps, ntypes, hydrogen, doDmap;
-  const float* table;             // [ntypes][kAffRows][G] for this pass
-  const float* tableH;            // [kAffRows][G] hydrogen rows for this pass, or null
+  int nmaps, nmPad, ntypes, hydrogen;
+  const float* table;             // [ntypes][kAffRows][nmPad] FP32
+  const float* tableH;            // [kAffRows][nmPad] rows of the "HD" type (disordered donors), or null
   const float* sol;               // kAffRows
-  int mapHbond[kAffMaxGroup], mapIsHB[kAffMaxGroup], mapCov[kAffMaxGroup];
-  float solparProbe[kAffMaxGroup], volProbe[kAffMaxGroup];
+  const double* thr;              // thr[k]: least r^2 whose reference bin int(100/(1/sqrt(r^2))) is >= k
+  float delta;                    // guard half-width around bin edges (units of 0.01 A)
+  int typeHbond[kMaxTypes];
+  unsigned typeModes[kMaxTypes];
+  int typeNeedsAngular[kMaxTypes];
+  int mapMinMaxSlot[kMaxMapsPass];
+  int mapCov[kMaxMapsPass];
+  float solparProbe[kMaxMapsPass], volProbe[kMaxMapsPass];
   float solparQ;
-  float* out;                     // [nmaps][npoints]
+  float* out;                     // this pass's first map: [nmaps][npoints]
   float* dmap;
   unsigned* status;
 };
 
-size_t aff_smem_bytes(int ntypes, int G);
+size_t aff_smem_bytes(int nmPad);
 cudaError_t aff_launch(const AffParams& P, cudaStream_t st);
 
 // Cell list build (counting sort of atoms into 8 A cells, file order kept inside each cell).

@@ -87,6 +87,35 @@ const std::vector<double>& binThresholds() {
   return thr;
 }
 
+// The same for the affinity pass, whose bin is int((1 / (1 / sqrt(r^2))) * 100)
+// (CalculateGridmaps.cpp:284-289): thr[k] is the least r^2 with bin >= k.
+const std::vector<double>& affinityBinThresholds() {
+  static std::vector<double> thr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    thr.assign(agk::kAffRows + 1, 0.0);
+    auto binOf = [](double r2) {
+      volatile double inv = 1.0 / sqrt(r2);
+      volatile double r = 1.0 / inv;
+      return r * 100.0;
+    };
+    for (int k = 1; k <= agk::kAffRows; k++) {
+      double lo = 0.0, hi = (k / 100.0 + 1.0) * (k / 100.0 + 1.0);
+      uint64_t a, b;
+      memcpy(&a, &lo, 8);
+      memcpy(&b, &hi, 8);
+      while (b - a > 1) {
+        uint64_t m = a + (b - a) / 2;
+        double v;
+        memcpy(&v, &m, 8);
+        if (binOf(v) >= (double)k) b = m; else a = m;
+      }
+      memcpy(&thr[k], &b, 8);
+    }
+  });
+  return thr;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -111,8 +140,17 @@ struct ag_ctx {
   double itemsH = 0;
   // affinity
   DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
-  DevBuf<float> vol, solq, affTab, affTabH, sol;
-  DevBuf<double> rv, rv2;
+  DevBuf<float> vol, solq, affTab, affTabH, sol, rv32, rv2_32;
+  DevBuf<double> rv64, thrA;
+  struct Pass {
+    int m0, nm, nmPad;
+    size_t tabOff, tabHOff;
+    unsigned typeModes[agk::kMaxTypes];
+    int typeNeedsAngular[agk::kMaxTypes];
+    int mapMinMaxSlot[agk::kMaxMapsPass];
+  };
+  std::vector<Pass> passes;
+  int typeHbond[agk::kMaxTypes] = {0};
   // job
   bool haveJob = false, haveAff = false, ddd = true;
   ag_grid grid{};
@@ -159,12 +197,13 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   if (!c) return AG_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
-  for (auto* b : {&c->epsTab, &c->maps, &c->vol, &c->solq, &c->affTab, &c->affTabH, &c->sol}) b->release();
+  for (auto* b : {&c->epsTab, &c->maps, &c->vol, &c->solq, &c->affTab, &c->affTabH, &c->sol, &c->rv32, &c->rv2_32})
+    b->release();
   c->atoms.release();
   c->thr.release();
   c->partial.release();
-  c->rv.release();
-  c->rv2.release();
+  c->rv64.release();
+  c->thrA.release();
   c->blocks.release();
   c->status.release();
   for (auto* b : {&c->items, &c->info, &c->cellStart, &c->cellAtoms, &c->cellOf, &c->count, &c->fill, &c->dStart,
@@ -199,12 +238,22 @@ void buildItems(ag_ctx* c) {
   const int nxc = (g.nx + agk::kNX - 1) / agk::kNX;
   const int TX = 2, TY = 16, TZ = 8;
   c->hItems.clear();
-  for (int tz = 0; tz < g.nz; tz += TZ)
-    for (int ty = 0; ty < g.ny; ty += TY)
-      for (int tx = 0; tx < nxc; tx += TX)
+  // Tiles in boustrophedon order (y rows and x columns reverse direction on
+  // alternate passes), so a CTA that continues from one tile into the next
+  // stays within neighbouring tiles and its box stays compact.
+  const int ntx = (nxc + TX - 1) / TX, nty = (g.ny + TY - 1) / TY, ntz = (g.nz + TZ - 1) / TZ;
+  int serp = 0;
+  for (int kz = 0; kz < ntz; kz++)
+    for (int ky0 = 0; ky0 < nty; ky0++) {
+      const int ky = (kz & 1) ? nty - 1 - ky0 : ky0;
+      for (int kx0 = 0; kx0 < ntx; kx0++, serp++) {
+        const int kx = (serp / ntx) & 1 ? ntx - 1 - kx0 : kx0;
+        const int tx = kx * TX, ty = ky * TY, tz = kz * TZ;
         for (int z = tz; z < std::min(g.nz, tz + TZ); z++)
           for (int y = ty; y < std::min(g.ny, ty + TY); y++)
             for (int x = tx; x < std::min(nxc, tx + TX); x++) c->hItems.push_back(x | (y << 8) | (z << 19));
+      }
+    }
   c->hBlocks.clear();
   const double h = g.spacing;
   const int n2x = g.nx / 2, n2y = g.ny / 2, n2z = g.nz / 2;
@@ -230,6 +279,12 @@ void buildItems(ag_ctx* c) {
     b.hx = (float)(50.0 * (hi[0] - lo[0]) + 1.0);
     b.hy = (float)(50.0 * (hi[1] - lo[1]) + 1.0);
     b.hz = (float)(50.0 * (hi[2] - lo[2]) + 1.0);
+    // Atoms at least rFar from the box use the saturated dielectric; nearer ones
+    // read the table, whose index then stays below 8191 without clamping.
+    const double diag = 2.0 * std::sqrt((double)b.hx * b.hx + (double)b.hy * b.hy + (double)b.hz * b.hz) / 100.0;
+    const double rFar = std::max(50.0, std::min(60.0, 81.0 - diag));
+    b.rfar2 = (float)((100.0 * rFar) * (100.0 * rFar));
+    b.clampMid = rFar + diag >= 81.0 ? 1 : 0;  // mid-list bins may then exceed the table
     c->hBlocks.push_back(b);
   }
   c->itemsFor[0] = g.nx;
@@ -325,15 +380,27 @@ int stageAffinity(ag_ctx* c, const ag_receptor* r, const ag_affinity_params* p) 
     vol[i] = (float)r->vol[i];
     solq[i] = (float)(r->solpar[i] + p->solpar_q * fabs(r->charge[i]));
   }
+  // The H-bond class is a property of the receptor type; the kernel branches on it per type.
+  for (int t = 0; t < agk::kMaxTypes; t++) c->typeHbond[t] = -1;
+  for (int i = 0; i < n; i++) {
+    int& th = c->typeHbond[r->type[i]];
+    if (th < 0) th = r->hbond[i];
+    else if (th != r->hbond[i])
+      return fail(AG_E_INVALID, "atoms of receptor type %d have different H-bond classes", r->type[i]);
+  }
+  for (int t = 0; t < agk::kMaxTypes; t++) if (c->typeHbond[t] < 0) c->typeHbond[t] = ag::NON;
+  std::vector<float> rv32(3 * (size_t)n), rv2_32(3 * (size_t)n);
+  for (size_t i = 0; i < 3 * (size_t)n; i++) { rv32[i] = (float)r->rvector[i]; rv2_32[i] = (float)r->rvector2[i]; }
   CK(c->info.ensure(n)); CK(c->donorMask.ensure(n)); CK(c->vol.ensure(n)); CK(c->solq.ensure(n));
-  CK(c->rv.ensure(3 * (size_t)n)); CK(c->rv2.ensure(3 * (size_t)n));
+  CK(c->rv32.ensure(3 * (size_t)n)); CK(c->rv2_32.ensure(3 * (size_t)n)); CK(c->rv64.ensure(3 * (size_t)n));
   if (n) {
     CK(cudaMemcpyAsync(c->info.p, info.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->donorMask.p, donor.data(), sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->vol.p, vol.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->solq.p, solq.data(), sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->rv.p, r->rvector, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->rv2.p, r->rvector2, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rv32.p, rv32.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rv2_32.p, rv2_32.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->rv64.p, r->rvector, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
   }
   c->nMaps = p->n_maps;
   c->nTypes = p->n_types;
@@ -344,32 +411,69 @@ int stageAffinity(ag_ctx* c, const ag_receptor* r, const ag_affinity_params* p) 
   c->mapCov.assign(p->map_is_covalent, p->map_is_covalent + p->n_maps);
   c->solparProbe.assign(p->solpar_probe, p->solpar_probe + p->n_maps);
   c->volProbe.assign(p->vol_probe, p->vol_probe + p->n_maps);
-  // Pair-energy tables, FP32, rows r <= 8 A, laid out per pass [type][row][G].
+
+  // Split the maps into passes of at most 16 maps and 4 min/max maps.
   const int nm = p->n_maps, nt = p->n_types;
-  std::vector<float> tab((size_t)nt * agk::kAffRows * std::max(nm, 1));
-  std::vector<float> tabH((size_t)agk::kAffRows * std::max(nm, 1));
-  int G = std::max(1, std::min(nm, agk::kAffMaxGroup));
-  while (G > 1 && agk::aff_smem_bytes(nt, G) > 100 * 1024) G--;
-  int npass = nm ? (nm + G - 1) / G : 0;
-  if (npass) G = (nm + npass - 1) / npass;
-  size_t off = 0;
-  for (int m0 = 0; m0 < nm; m0 += G) {
-    int g = std::min(G, nm - m0);
+  auto isMinMax = [&](int m) {
+    const int hb = c->mapHbond[m];
+    return c->mapIsHB[m] && !c->mapCov[m] && (hb == ag::A1 || hb == ag::DS || hb == ag::D1);
+  };
+  c->passes.clear();
+  for (int m0 = 0; m0 < nm;) {
+    ag_ctx::Pass ps{};
+    ps.m0 = m0;
+    int mm = 0, k = 0;
+    while (m0 + k < nm && k < agk::kMaxMapsPass) {
+      if (isMinMax(m0 + k) && mm == agk::kMaxMinMax) break;
+      ps.mapMinMaxSlot[k] = isMinMax(m0 + k) ? mm++ : -1;
+      k++;
+    }
+    ps.nm = k;
+    ps.nmPad = ((k + 3) / 4) * 4;
+    for (int t = 0; t < nt; t++) {
+      unsigned modes = 0;
+      const int ahb = c->typeHbond[t];
+      const bool donor = ahb == ag::DS || ahb == ag::D1;
+      for (int g = 0; g < k; g++) {
+        const int m = m0 + g, mhb = c->mapHbond[m];
+        unsigned mode = 0;
+        if (c->mapIsHB[m] && !c->mapCov[m]) {
+          if ((mhb == ag::AS || mhb == ag::A2) && donor) mode = 1;
+          else if (mhb == ag::A1 && donor) mode = 2;
+          else if ((mhb == ag::DS || mhb == ag::D1) && ahb >= ag::AS) mode = 3;
+        }
+        modes |= mode << (2 * g);
+      }
+      ps.typeModes[t] = modes;
+      ps.typeNeedsAngular[t] = modes != 0 && (ahb == ag::D1 || ahb == ag::A1 || ahb == ag::A2);
+    }
+    c->passes.push_back(ps);
+    m0 += k;
+  }
+  // Pair-energy tables, FP32, rows r <= 8 A, per pass [type][row][nmPad].
+  size_t tabSize = 0, tabHSize = 0;
+  for (auto& ps : c->passes) {
+    ps.tabOff = tabSize;
+    ps.tabHOff = tabHSize;
+    tabSize += (size_t)nt * agk::kAffRows * ps.nmPad;
+    tabHSize += (size_t)agk::kAffRows * ps.nmPad;
+  }
+  std::vector<float> tab(std::max<size_t>(tabSize, 4), 0.f), tabH(std::max<size_t>(tabHSize, 4), 0.f);
+  for (auto& ps : c->passes) {
     for (int t = 0; t < nt; t++)
       for (int i = 0; i < agk::kAffRows; i++)
-        for (int k = 0; k < g; k++)
-          tab[off + ((size_t)t * agk::kAffRows + i) * g + k] = (float)p->energy[((size_t)t * 8192 + i) * nm + m0 + k];
-    off += (size_t)nt * agk::kAffRows * g;
-  }
-  off = 0;
-  if (p->hydrogen >= 0 && p->hydrogen < nt) {
-    for (int m0 = 0; m0 < nm; m0 += G) {
-      int g = std::min(G, nm - m0);
+        for (int g = 0; g < ps.nm; g++)
+          tab[ps.tabOff + ((size_t)t * agk::kAffRows + i) * ps.nmPad + g] =
+              (float)p->energy[((size_t)t * 8192 + i) * nm + ps.m0 + g];
+    if (p->hydrogen >= 0 && p->hydrogen < nt)
       for (int i = 0; i < agk::kAffRows; i++)
-        for (int k = 0; k < g; k++)
-          tabH[off + (size_t)i * g + k] = (float)p->energy[((size_t)p->hydrogen * 8192 + i) * nm + m0 + k];
-      off += (size_t)agk::kAffRows * g;
-    }
+        for (int g = 0; g < ps.nm; g++)
+          tabH[ps.tabHOff + (size_t)i * ps.nmPad + g] = (float)p->energy[((size_t)p->hydrogen * 8192 + i) * nm + ps.m0 + g];
+  }
+  if (!c->thrA.p) {
+    const auto& thr = affinityBinThresholds();
+    CK(c->thrA.ensure(thr.size()));
+    CK(cudaMemcpyAsync(c->thrA.p, thr.data(), sizeof(double) * thr.size(), cudaMemcpyHostToDevice, c->stream));
   }
   std::vector<float> sol(agk::kAffRows);
   for (int i = 0; i < agk::kAffRows; i++) sol[i] = (float)p->sol[i];
@@ -418,42 +522,46 @@ int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
   CK(agk::closest_h_launch(H, c->stream));
   c->launches += 1;
 
-  const int nm = c->nMaps, nt = c->nTypes;
-  int G = std::max(1, std::min(nm, agk::kAffMaxGroup));
-  while (G > 1 && agk::aff_smem_bytes(nt, G) > 100 * 1024) G--;
-  int npass = nm ? (nm + G - 1) / G : 0;
-  if (npass) G = (nm + npass - 1) / npass;
-  size_t off = 0, offH = 0;
-  for (int m0 = 0, pass = 0; m0 < nm || (nm == 0 && pass == 0); m0 += std::max(G, 1), pass++) {
-    const int gsz = nm ? std::min(G, nm - m0) : 0;
+  const int nt = c->nTypes;
+  std::vector<ag_ctx::Pass> passes = c->passes;
+  if (passes.empty()) {  // no ligand maps: one pass for the d-map alone
+    ag_ctx::Pass ps{};
+    ps.nmPad = 4;
+    for (int k = 0; k < agk::kMaxMapsPass; k++) ps.mapMinMaxSlot[k] = -1;
+    passes.push_back(ps);
+  }
+  for (const auto& ps : passes) {
     agk::AffParams P{};
     P.n_atoms = n; P.xyz = c->atoms.p; P.info = c->info.p; P.vol = c->vol.p; P.solq = c->solq.p;
-    P.rv = c->rv.p; P.rv2 = c->rv2.p;
+    P.rv = c->rv32.p; P.rv2 = c->rv2_32.p; P.rv64 = c->rv64.p;
     P.cellStart = c->cellStart.p; P.cellAtoms = c->cellAtoms.p;
     for (int d = 0; d < 3; d++) { P.cellLo[d] = lo[d]; P.ncell[d] = ncell[d]; }
     P.closestH = c->closestH.p;
     P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.n2x = g.nx / 2; P.n2y = g.ny / 2; P.n2z = g.nz / 2;
     P.npoints = np; P.h = h;
-    P.m0 = m0; P.G = gsz; P.nmaps = nm; P.ntypes = nt; P.hydrogen = c->hydrogen; P.doDmap = pass == 0;
-    P.table = c->affTab.p + off;
-    P.tableH = (c->hydrogen >= 0 && c->hydrogen < nt) ? c->affTabH.p + offH : nullptr;
+    P.nmaps = ps.nm; P.nmPad = ps.nmPad; P.ntypes = nt; P.hydrogen = c->hydrogen;
+    P.table = c->affTab.p + ps.tabOff;
+    P.tableH = (c->hydrogen >= 0 && c->hydrogen < nt) ? c->affTabH.p + ps.tabHOff : nullptr;
     P.sol = c->sol.p;
-    for (int k = 0; k < gsz; k++) {
-      P.mapHbond[k] = c->mapHbond[m0 + k];
-      P.mapIsHB[k] = c->mapIsHB[m0 + k];
-      P.mapCov[k] = c->mapCov[m0 + k];
-      P.solparProbe[k] = c->solparProbe[m0 + k];
-      P.volProbe[k] = c->volProbe[m0 + k];
+    P.thr = c->thrA.p;
+    P.delta = 1.0e-3f;
+    for (int t = 0; t < agk::kMaxTypes; t++) {
+      P.typeHbond[t] = c->typeHbond[t];
+      P.typeModes[t] = ps.typeModes[t];
+      P.typeNeedsAngular[t] = ps.typeNeedsAngular[t];
+    }
+    for (int k = 0; k < agk::kMaxMapsPass; k++) {
+      P.mapMinMaxSlot[k] = k < ps.nm ? ps.mapMinMaxSlot[k] : -1;
+      P.mapCov[k] = k < ps.nm ? c->mapCov[ps.m0 + k] : 1;
+      P.solparProbe[k] = k < ps.nm ? (float)c->solparProbe[ps.m0 + k] : 0.f;
+      P.volProbe[k] = k < ps.nm ? (float)c->volProbe[ps.m0 + k] : 0.f;
     }
     P.solparQ = (float)c->solparQ;
-    P.out = dMaps;
+    P.out = dMaps + (size_t)ps.m0 * np;
     P.dmap = dDmap;
     P.status = c->status.p;
     CK(agk::aff_launch(P, c->stream));
     c->launches += 1;
-    off += (size_t)nt * agk::kAffRows * gsz;
-    offH += (size_t)agk::kAffRows * gsz;
-    if (nm == 0) break;
   }
   return AG_OK;
 }

@@ -4,8 +4,8 @@
 //
 // (FastGrid electrostatics/Cpu.cpp:27-88; the table is InputDataLoader.cpp:
 // 715-742).  There is no cutoff, so the work is N_atoms x N_points pairs and
-// the kernel is bound by the SM's issue rate (one SFU rsqrt, one shared-memory
-// table read and ~10 FP32 ops per pair), not by HBM.
+// the kernel is bound by the SM's instruction issue (one SFU rsqrt, one
+// shared-memory table read and ~6 FP32/INT ops per pair), not by HBM.
 //
 // Layout and schedule
 //  * Work item = NX consecutive x points of one (y, z) row; one thread per item,
@@ -14,17 +14,20 @@
 //    records, fetched with 1-D TMA bulk copies into a two-slot ring and
 //    tracked by mbarriers (no multicast).
 //  * Each tile is converted once per CTA to CTA-local coordinates scaled by
-//    100 (so 100*r comes straight out of r^2 * rsqrt(r^2)) and split into
-//    "near" atoms (closer than rNear to the CTA's box) and "far" atoms.
-//  * Far pairs: floor(100 r) by a round-toward-minus-infinity FMA, table read
-//    from shared memory, Kahan-compensated FP32 sum.
-//  * Near pairs additionally clamp 1/r at 2 and check whether 100 r lies within
-//    `delta` of a bin edge; if so the bin is decided exactly in FP64 against
-//    a table of squared-distance thresholds, so the step-function table is
-//    indexed exactly as the reference's FP64 code indexes it.
-//  * Tile sums are added into per-point FP64 accumulators.  When the grid is
-//    too small to fill the GPU, atoms are split across CTAs and the FP64
-//    partial sums are reduced in a fixed order by a second kernel.
+//    100 (so 100 r comes straight out of r^2 * rsqrt(r^2)) and split by the
+//    atom's distance d to the CTA's box into three lists:
+//      near (d < rNear): 1/r capped at 2, Kahan-compensated per pair, and the
+//        bin decided exactly in FP64 (squared-distance threshold table) when
+//        100 r lies within `delta` of a bin edge;
+//      mid (rNear <= d < rFar): bin by a round-down FMA, table read;
+//      far (d >= rFar, at least 50 A): the table has saturated there (its
+//        entries differ from entry 8191 by < 2e-6 relative), so the term is
+//        w * invEps[8191] / r with no table read.
+//    Mid and far terms are summed in plain FP32 over chunks of kChunk atoms
+//    and the chunk sums are Kahan-compensated.
+//  * When the grid is too small to fill the GPU, atoms are split across CTAs
+//    and the per-CTA results are reduced in FP64, in a fixed order, by a
+//    second kernel.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -39,14 +42,16 @@ using namespace agd;
 constexpr int kThreads = 256;
 constexpr int kTile = 256;        // atoms per shared-memory tile
 constexpr int kTabLen = 8192;     // invEps entries
+constexpr int kChunk = 32;        // atoms per plain-FP32 chunk sum
 
 struct EmapSmem {
   float tab[kTabLen];             // 32 KB
   double4 ring[2][kTile];         // 16 KB, TMA destination
   float4 nearA[kTile];            // local scaled x, y, z and 100*w
-  float4 farA[kTile];
+  float4 midA[kTile];
+  float4 farA[kTile];             // w pre-multiplied by invEps[8191]
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
-  int cnt[2][kThreads / 32];
+  int cnt[3][kThreads / 32];
   uint64_t bar[2];
 };
 
@@ -54,6 +59,56 @@ __device__ __forceinline__ void unpack_item(int v, int& xc, int& y, int& z) {
   xc = v & 0xFF;
   y = (v >> 8) & 0x7FF;
   z = (v >> 19) & 0x7FF;
+}
+
+template <int MODE>
+__device__ __forceinline__ void add_chunk(float (&sum)[kNX], float (&cmp)[kNX], const float (&cs)[kNX]) {
+  if (MODE == kEmapKahan) {
+#pragma unroll
+    for (int k = 0; k < kNX; k++) {
+      const float y = cs[k] - cmp[k];
+      const float s1 = sum[k] + y;
+      cmp[k] = (s1 - sum[k]) - y;
+      sum[k] = s1;
+    }
+  }
+}
+
+// Mid-list atoms: bin by a round-down FMA, table read, plain FP32 chunk sums.
+// CLAMP: the CTA's box is large enough that a bin can pass the table's end.
+template <int MODE, bool CLAMP>
+__device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, const float* __restrict__ tab, int n,
+                                          const float (&gx)[kNX], float gy, float gz, float (&sum)[kNX],
+                                          float (&cmp)[kNX]) {
+  const float kBias = 8388608.f;
+#pragma unroll 1
+  for (int j0 = 0; j0 < n; j0 += kChunk) {
+    float cs[kNX];
+#pragma unroll
+    for (int k = 0; k < kNX; k++) cs[k] = (MODE == kEmapKahan) ? 0.f : sum[k];
+    const int j1 = min(n, j0 + kChunk);
+#pragma unroll 1
+    for (int j = j0; j < j1; j++) {
+      const float4 a = list[j];
+      const float dy = a.y - gy, dz = a.z - gz;
+      const float dyz2 = fmaf(dz, dz, dy * dy);
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        const float dx = a.x - gx[k];
+        const float r2 = fmaf(dx, dx, dyz2);
+        const float rs = rsqrt_approx(r2);
+        float f = __fmaf_rd(r2, rs, kBias);
+        if (CLAMP) f = fminf(f, kBias + (float)(kTabLen - 1));
+        cs[k] = fmaf(a.w * rs, tab[__float_as_int(f) - 0x4B000000], cs[k]);
+      }
+    }
+    if (MODE == kEmapKahan) {
+      add_chunk<MODE>(sum, cmp, cs);
+    } else {
+#pragma unroll
+      for (int k = 0; k < kNX; k++) sum[k] = cs[k];
+    }
+  }
 }
 
 template <bool DDD, int MODE>
@@ -90,18 +145,18 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
     fence_barrier_init();
   }
   __syncthreads();
+  const float gFar = DDD ? S.tab[kTabLen - 1] : 1.f;
   if (tid == 0 && ntiles > 0) {
     unsigned n0 = (unsigned)min(kTile, a1 - a0);
     mbar_arrive_expect_tx(&S.bar[0], n0 * 32u);
     tma_load_1d(S.ring[0], P.atoms + a0, n0 * 32u, &S.bar[0]);
   }
 
-  double acc[kNX];
   float sum[kNX], cmp[kNX];
 #pragma unroll
-  for (int k = 0; k < kNX; k++) { acc[k] = 0.0; sum[k] = 0.f; cmp[k] = 0.f; }
+  for (int k = 0; k < kNX; k++) { sum[k] = 0.f; cmp[k] = 0.f; }
 
-  const float cap = 0.02f;  // min(1/r, 2) in units of 1/(100 r)
+  const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
   const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
 
   for (int t = 0; t < ntiles; t++) {
@@ -128,70 +183,73 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
     }
 
     // Classify and convert this tile's atoms (one atom per thread).
-    bool isNear = false;
+    int cls = -1;  // 0 near, 1 mid, 2 far
     float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
-    const bool have = tid < nt;
-    if (have) {
+    if (tid < nt) {
       double4 a = S.ring[slot][tid];
       loc.x = (float)((a.x - B.ox) * 100.0);
       loc.y = (float)((a.y - B.oy) * 100.0);
       loc.z = (float)((a.z - B.oz) * 100.0);
       loc.w = (float)(a.w * 100.0);
-      float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
-            dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
-      isNear = dx * dx + dy * dy + dz * dz < P.rnear2;
+      const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
+                  dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
+      const float d2 = dx * dx + dy * dy + dz * dz;
+      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? 1 : 2);
+      if (cls == 2) loc.w *= gFar;
     }
-    const unsigned nb = __ballot_sync(0xffffffffu, have && isNear);
-    const unsigned fb = __ballot_sync(0xffffffffu, have && !isNear);
-    if (lane == 0) { S.cnt[0][warp] = __popc(nb); S.cnt[1][warp] = __popc(fb); }
+    const unsigned b0 = __ballot_sync(0xffffffffu, cls == 0);
+    const unsigned b1 = __ballot_sync(0xffffffffu, cls == 1);
+    const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
+    if (lane == 0) { S.cnt[0][warp] = __popc(b0); S.cnt[1][warp] = __popc(b1); S.cnt[2][warp] = __popc(b2); }
     __syncthreads();
-    int nNear = 0, nFar = 0, offN = 0, offF = 0;
+    int nNear = 0, nMid = 0, nFar = 0, off0 = 0, off1 = 0, off2 = 0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) {
-      if (w == warp) { offN = nNear; offF = nFar; }
+      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; }
       nNear += S.cnt[0][w];
-      nFar += S.cnt[1][w];
+      nMid += S.cnt[1][w];
+      nFar += S.cnt[2][w];
     }
     const unsigned lt = (1u << lane) - 1u;
-    if (have) {
-      if (isNear) {
-        int pos = offN + __popc(nb & lt);
-        S.nearA[pos] = loc;
-        S.nearIdx[pos] = (short)tid;
-      } else {
-        S.farA[offF + __popc(fb & lt)] = loc;
-      }
+    if (cls == 0) {
+      const int pos = off0 + __popc(b0 & lt);
+      S.nearA[pos] = loc;
+      S.nearIdx[pos] = (short)tid;
+    } else if (cls == 1) {
+      S.midA[off1 + __popc(b1 & lt)] = loc;
+    } else if (cls == 2) {
+      S.farA[off2 + __popc(b2 & lt)] = loc;
     }
     __syncthreads();
 
-    // Far atoms.
+    // Mid atoms: table read, plain FP32 within a chunk.
+    if (DDD) {
+      if (B.clampMid) mid_atoms<MODE, true>(S.midA, S.tab, nMid, gx, gy, gz, sum, cmp);
+      else mid_atoms<MODE, false>(S.midA, S.tab, nMid, gx, gy, gz, sum, cmp);
+    }
+
+    // Far atoms: saturated dielectric (or the constant dielectric), no table.
 #pragma unroll 1
-    for (int j = 0; j < nFar; j++) {
-      const float4 a = S.farA[j];
-      const float dy = a.y - gy, dz = a.z - gz;
-      const float dyz2 = fmaf(dz, dz, dy * dy);
+    for (int j0 = 0; j0 < nFar; j0 += kChunk) {
+      float cs[kNX];
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        const float dx = a.x - gx[k];
-        const float r2 = fmaf(dx, dx, dyz2);
-        const float rs = rsqrt_approx(r2);
-        float term;
-        if (DDD) {
-          float f = __fmaf_rd(r2, rs, kBias);
-          f = fminf(f, kBias + (float)(kTabLen - 1));
-          term = (a.w * rs) * S.tab[__float_as_int(f) - 0x4B000000];
-        } else {
-          term = a.w * rs;
-        }
-        if (MODE == kEmapKahan) {
-          const float y = term - cmp[k];
-          const float s1 = sum[k] + y;
-          cmp[k] = (s1 - sum[k]) - y;
-          sum[k] = s1;
-        } else {
-          sum[k] += term;
+      for (int k = 0; k < kNX; k++) cs[k] = (MODE == kEmapKahan) ? 0.f : sum[k];
+      const int j1 = min(nFar, j0 + kChunk);
+#pragma unroll 1
+      for (int j = j0; j < j1; j++) {
+        const float4 a = S.farA[j];
+        const float dy = a.y - gy, dz = a.z - gz;
+        const float dyz2 = fmaf(dz, dz, dy * dy);
+#pragma unroll
+        for (int k = 0; k < kNX; k++) {
+          const float dx = a.x - gx[k];
+          cs[k] = fmaf(a.w, rsqrt_approx(fmaf(dx, dx, dyz2)), cs[k]);
         }
       }
+      if (MODE == kEmapKahan) add_chunk<MODE>(sum, cmp, cs);
+      else
+#pragma unroll
+        for (int k = 0; k < kNX; k++) sum[k] = cs[k];
     }
 
     // Near atoms: clamp 1/r at 2 and decide bins near an edge exactly.
@@ -251,15 +309,6 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
         }
       }
     }
-
-    if (MODE == kEmapKahan) {
-#pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        acc[k] += (double)sum[k] - (double)cmp[k];
-        sum[k] = 0.f;
-        cmp[k] = 0.f;
-      }
-    }
     __syncthreads();  // ring slot and atom lists are free again
   }
 
@@ -269,7 +318,7 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
   for (int k = 0; k < kNX; k++) {
     const int x = xc * kNX + k;
     if (x >= P.nx) break;
-    const double v = (MODE == kEmapKahan) ? acc[k] : (double)sum[k];
+    const double v = (MODE == kEmapKahan) ? (double)sum[k] - (double)cmp[k] : (double)sum[k];
     if (P.nsplit == 1)
       P.out[row + x] = (float)v;
     else
@@ -277,7 +326,7 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
   }
 }
 
-// Sum the atom-split partials in split order.
+// Sum the atom-split partials in split order (FP64).
 __global__ void emap_reduce_kernel(const double* __restrict__ partial, int nsplit, int64_t n, float* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;

@@ -163,6 +163,11 @@ int ag_problem_write(ag_problem* p);
 /* The autogrid4 / fastgrid4 command line (ProgramParameters.cpp:63-112). */
 int ag_main(int argc, char** argv);
 
+/* Measured issue-rate peaks of a device (no reference counterpart; used for
+ * the e-map's roofline): SFU reciprocal square roots per second and FP32 FMA
+ * instructions per second, at the clocks the device runs at now. */
+int ag_measure_peaks(int device, double* rsqrt_per_s, double* ffma_per_s);
+
 /* ------------------------------------------------------------------------ */
 /* Seeded synthetic receptors for tests and benchmarks: a self-avoiding      */
 /* chain walk inside a sphere or ellipsoid, AutoDock4 types by fraction,     */
