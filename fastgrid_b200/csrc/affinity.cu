@@ -23,13 +23,14 @@
 //   S1 = sum sol(r) vol_a,  S2 = sum sol(r) (solpar_a + solparQ |q_a|),
 // so map m receives solparProbe_m S1 + volProbe_m S2 and the d-map solparQ S1.
 //
-// Schedule.  One CTA per 8x8x4 block of points, one point per thread.  The
-// CTA gathers the atoms of the 8 A cells around its box that lie within 8 A of
-// the box (shared memory, batches of kCap), orders them by receptor type, and
-// walks one type at a time with that type's FP32 table rows (801 x nmPad) in
-// shared memory, fetched by TMA bulk copies into two buffers so the next
-// type's rows load while the current type is processed.  All branches on the
-// atom's H-bond class and the map's H-bond mode are uniform across the CTA.
+// Schedule.  One CTA per 8x8x4 block of points, one point per thread.  The CTA
+// lists the 8 A cells around its box, prefix-sums their atom counts, and
+// gathers the atoms within 8 A of the box 256 at a time into a shared-memory
+// batch (up to kCap).  A batch is ordered by receptor type and walked one type
+// at a time with that type's FP32 table rows (801 x nmPad) in shared memory,
+// fetched by TMA bulk copies into two buffers so the next type's rows load
+// while the current type is processed.  Branches on the atom's H-bond class
+// and the map's H-bond mode are uniform across the CTA.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -42,7 +43,8 @@ namespace agk {
 using namespace agd;
 
 constexpr int kAffThreads = kAffTX * kAffTY * kAffTZ;  // 256
-constexpr int kCap = 384;                              // candidate atoms per batch
+constexpr int kCap = 512;                              // candidate atoms per batch
+constexpr int kMaxCells = 128;                         // cells per gather group
 enum { NON = 0, DS = 1, D1 = 2, AS = 3, A1 = 4, A2 = 5 };
 #define AG_PI 3.14159265358979323846
 
@@ -57,11 +59,12 @@ struct CandF {          // FP32 view, CTA-local coordinates
 
 struct AffSmem {
   CandF cand[kCap];
-  double cx[kCap], cy[kCap], cz[kCap];  // FP64 grid-centred coordinates (exact fallbacks)
   short perm[kCap];
   int typeStart[kMaxTypes + 1];
   int run[kMaxTypes + 1];
   int cnt[kAffThreads / 32];
+  int cellBeg[kMaxCells];
+  int cellPre[kMaxCells + 1];
   float sol[kAffRows + 3];
   uint64_t bar[2];
 };
@@ -97,6 +100,7 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nmPad = P.nmPad;
   const unsigned tabBytes = (unsigned)(kAffRows * nmPad * sizeof(float));
+  const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
 
   // This CTA's block of points and this thread's point.
   const int tbx = (P.nx + kAffTX - 1) / kAffTX, tby = (P.ny + kAffTY - 1) / kAffTY;
@@ -119,6 +123,7 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
   lo[1] = oy; hi[1] = (double)(min(y0 + kAffTY, P.ny) - 1 - P.n2y) * h;
   lo[2] = oz; hi[2] = (double)(min(z0 + kAffTZ, P.nz) - 1 - P.n2z) * h;
   int c0[3], c1[3];
+#pragma unroll
   for (int d = 0; d < 3; d++) {
     c0[d] = max(0, (int)floor((lo[d] - 8.0 - P.cellLo[d]) / 8.0));
     c1[d] = min(P.ncell[d] - 1, (int)floor((hi[d] + 8.0 - P.cellLo[d]) / 8.0));
@@ -142,62 +147,13 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
   for (int s = 0; s < kMaxMinMax; s++) { mn[s] = 999999.f; mx[s] = -999999.f; }
   unsigned mmFlag = 0;
   float S1 = 0.f, S2 = 0.f;
+  unsigned phaseBits = 0u;   // phase of the two table buffers' barriers (bit b = buffer b)
+  bool aborted = false;
+  int nb = 0;                // candidates in the current batch
 
-  const int ncx = c1[0] - c0[0] + 1, ncy = c1[1] - c0[1] + 1, ncz = c1[2] - c0[2] + 1;
-  const int ncells = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy * ncz : 0;
-  int ci = 0, pos = 0;
-  unsigned phaseBits = 0u;
-  __syncthreads();
-  while (ci < ncells) {
-    // ---- gather one batch of candidates (file order within cells) ----
-    int nb = 0;
-    while (ci < ncells) {
-      const int cx = c0[0] + ci % ncx, cy = c0[1] + (ci / ncx) % ncy, cz = c0[2] + ci / (ncx * ncy);
-      const int cell = (cz * P.ncell[1] + cy) * P.ncell[0] + cx;
-      const int cbeg = P.cellStart[cell], cend = P.cellStart[cell + 1];
-      const int cnt = min(cend - (cbeg + pos), kAffThreads);
-      if (cnt <= 0) { ci++; pos = 0; continue; }
-      if (nb + cnt > kCap) break;
-      bool keep = false;
-      int atom = -1;
-      double4 a = make_double4(0, 0, 0, 0);
-      if (tid < cnt) {
-        atom = P.cellAtoms[cbeg + pos + tid];
-        a = P.xyz[atom];
-        const double ddx = fmax(fmax(lo[0] - a.x, a.x - hi[0]), 0.0);
-        const double ddy = fmax(fmax(lo[1] - a.y, a.y - hi[1]), 0.0);
-        const double ddz = fmax(fmax(lo[2] - a.z, a.z - hi[2]), 0.0);
-        keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.001;
-      }
-      const unsigned kb = __ballot_sync(0xffffffffu, keep);
-      if (lane == 0) S.cnt[warp] = __popc(kb);
-      __syncthreads();
-      int total = 0, off = 0;
-#pragma unroll
-      for (int w = 0; w < kAffThreads / 32; w++) {
-        if (w == warp) off = total;
-        total += S.cnt[w];
-      }
-      if (keep) {
-        const int j = nb + off + __popc(kb & ((1u << lane) - 1u));
-        CandF& c = S.cand[j];
-        c.x = (float)(a.x - ox); c.y = (float)(a.y - oy); c.z = (float)(a.z - oz);
-        c.idx = atom;
-        c.vol = P.vol[atom];
-        c.solq = P.solq[atom];
-        c.info = P.info[atom];
-        c.rv[0] = P.rv[3 * atom]; c.rv[1] = P.rv[3 * atom + 1]; c.rv[2] = P.rv[3 * atom + 2];
-        c.rv2[0] = P.rv2[3 * atom]; c.rv2[1] = P.rv2[3 * atom + 1]; c.rv2[2] = P.rv2[3 * atom + 2];
-        S.cx[j] = a.x; S.cy[j] = a.y; S.cz[j] = a.z;
-      }
-      nb += total;
-      pos += cnt;
-      if (cbeg + pos >= cend) { ci++; pos = 0; }
-      __syncthreads();
-    }
-
-    // ---- order the batch by receptor type (stable counting sort, one warp) ----
-    if (warp == 0) {
+  // ---- one batch: order by receptor type, walk the types ----
+  auto processBatch = [&]() {
+    if (warp == 0) {  // stable counting sort by type, one warp
       for (int t = lane; t <= kMaxTypes; t += 32) S.run[t] = 0;
       __syncwarp();
       for (int base = 0; base < nb; base += 32) {
@@ -229,7 +185,6 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
     }
     __syncthreads();
 
-    // ---- walk the batch one receptor type at a time ----
     int slot = 0;
     int t = 0;
     while (t < P.ntypes && S.typeStart[t + 1] == S.typeStart[t]) t++;
@@ -247,17 +202,17 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
         tma_load_1d(tabBuf + (size_t)(slot ^ 1) * kAffRows * nmPad, P.table + (size_t)tn * kAffRows * nmPad, tabBytes,
                     &S.bar[slot ^ 1]);
       }
-      // Phase bits of the two buffers' barriers, kept in one word (bit b = buffer b).
       const bool ok = mbar_wait_bounded(&S.bar[slot], (phaseBits >> slot) & 1u, P.status);
       phaseBits ^= 1u << slot;
       if (__syncthreads_or(!ok)) {
         if (tid == 0 && tn < P.ntypes) mbar_wait_bounded(&S.bar[slot ^ 1], (phaseBits >> (slot ^ 1)) & 1u, P.status);
+        aborted = true;
         return;
       }
       const float* tab = tabBuf + (size_t)slot * kAffRows * nmPad;
       const int hb = P.typeHbond[t];
       const bool skipDisH = (t == P.hydrogen);
-      const unsigned modes = P.typeModes[t];       // 2 bits per map
+      const unsigned modes = P.typeModes[t];  // 2 bits per map
       const bool needAng = P.typeNeedsAngular[t];
 
       if (valid) {
@@ -271,17 +226,24 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
           if (skipDisH && dis) continue;
           double rSq64 = -1.0;
           if (r2 > 63.9998f) {
-            rSq64 = rsq_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz);
+            const double4 a64 = P.xyz[a.idx];
+            rSq64 = rsq_exact(a64.x, a64.y, a64.z, gx, gy, gz);
             if (rSq64 > 64.0) continue;
           }
           r2 = fmaxf(r2, 1.0e-24f);
           const float rs = rsqrt_approx(r2);
-          const float T = r2 * (rs * 100.f);
-          const float kr = (T + 12582912.f) - 12582912.f;
-          int iR = min((int)__fmaf_rd(r2, rs * 100.f, 0.f), kAffRows - 1);
+          const float rs100 = rs * 100.f;
+          const float T = r2 * rs100;
+          int iR = __float_as_int(__fmaf_rd(r2, rs100, kBias)) - 0x4B000000;
+          iR = min(iR, kAffRows - 1);
+          const float kb = T + 12582912.f;  // 1.5 * 2^23: nearest integer in the low bits
+          const float kr = kb - 12582912.f;
           if (fabsf(T - kr) < P.delta && kr >= 1.f && kr <= (float)(kAffRows - 1)) {
-            if (rSq64 < 0.0) rSq64 = rsq_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz);
-            const int k = (int)kr;
+            if (rSq64 < 0.0) {
+              const double4 a64 = P.xyz[a.idx];
+              rSq64 = rsq_exact(a64.x, a64.y, a64.z, gx, gy, gz);
+            }
+            const int k = __float_as_int(kb) - 0x4B400000;
             iR = (rSq64 >= P.thr[k]) ? k : k - 1;
           }
           const float ux = dx * rs, uy = dy * rs, uz = dz * rs;
@@ -294,7 +256,8 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
             if ((hb == D1 || (hb == A2 && !dis)) && fabsf(cosT) < 1.0e-5f) {
               // The D1 and ordered-A2 factors jump where cos(theta) changes sign:
               // take the sign from the reference's FP64 expression.
-              const double c64 = costheta_exact(S.cx[j], S.cy[j], S.cz[j], gx, gy, gz, P.rv64 + 3 * a.idx);
+              const double4 a64 = P.xyz[a.idx];
+              const double c64 = costheta_exact(a64.x, a64.y, a64.z, gx, gy, gz, P.rv64 + 3 * a.idx);
               cosT = (float)c64;
               gt0 = c64 > 0.0;
               ge0 = c64 >= 0.0;
@@ -350,12 +313,13 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
           const float sv = S.sol[iR];
           S1 = fmaf(sv, a.vol, S1);
           S2 = fmaf(sv, a.solq, S2);
-          const float* row = tab + iR * nmPad;
-          const float wAcc = Hramp, fAcc = racc, fDon = rdon;
+          const float4* row4 = reinterpret_cast<const float4*>(tab + iR * nmPad);
+          float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
           for (int g = 0; g < NMAX; g++) {
             if (g >= P.nmaps) break;
-            const float pwi = row[g];
+            if ((g & 3) == 0) q4 = row4[g >> 2];
+            const float pwi = (g & 3) == 0 ? q4.x : (g & 3) == 1 ? q4.y : (g & 3) == 2 ? q4.z : q4.w;
             const unsigned mode = (modes >> (2 * g)) & 3u;
             if (mode == 0u) {
               em[g] += pwi;
@@ -363,18 +327,18 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
               const float rsph = fminf(fmaxf(pwi * 0.01f, 0.f), 1.f);
               if (mode == 1u) {
                 const float e = dis ? (P.tableH ? P.tableH[max(0, iR - 110) * nmPad + g] : 0.f) : pwi;
-                em[g] += e * wAcc * (fAcc + (1.f - fAcc) * rsph);
+                em[g] += e * Hramp * (racc + (1.f - racc) * rsph);
               } else {
-                const float f = (mode == 2u) ? fAcc : fDon;
+                const float f = (mode == 2u) ? racc : rdon;
                 const float v = pwi * (f + (1.f - f) * rsph);
-                const int slot = P.mapMinMaxSlot[g];
+                const int mslot = P.mapMinMaxSlot[g];
 #pragma unroll
                 for (int s = 0; s < kMaxMinMax; s++)
-                  if (s == slot) {
+                  if (s == mslot) {
                     mn[s] = fminf(mn[s], v);
                     mx[s] = fmaxf(mx[s], v);
                   }
-                mmFlag |= 1u << slot;
+                mmFlag |= 1u << mslot;
               }
             }
           }
@@ -384,6 +348,100 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
       slot ^= 1;
       t = tn;
     }
+    nb = 0;
+  };
+
+  // ---- gather: cells around the box, 256 atoms per step ----
+  const int ncx = c1[0] - c0[0] + 1, ncy = c1[1] - c0[1] + 1, ncz = c1[2] - c0[2] + 1;
+  const int ncells = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy * ncz : 0;
+  for (int cg = 0; cg < ncells; cg += kMaxCells) {
+    const int ncg = min(kMaxCells, ncells - cg);
+    __syncthreads();  // the previous group's cell ranges are no longer read
+    if (warp == 0) {
+      constexpr int kPer = kMaxCells / 32;
+      int cnts[kPer];
+      int mine = 0;
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const int i = lane * kPer + q;
+        int c = 0;
+        if (i < ncg) {
+          const int ci = cg + i;
+          const int cx = c0[0] + ci % ncx, cy = c0[1] + (ci / ncx) % ncy, cz = c0[2] + ci / (ncx * ncy);
+          const int cell = (cz * P.ncell[1] + cy) * P.ncell[0] + cx;
+          const int beg = P.cellStart[cell];
+          c = P.cellStart[cell + 1] - beg;
+          S.cellBeg[i] = beg;
+        }
+        cnts[q] = c;
+        mine += c;
+      }
+      int incl = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int run = incl - mine;
+#pragma unroll
+      for (int q = 0; q < kPer; q++) {
+        const int i = lane * kPer + q;
+        if (i < ncg) S.cellPre[i] = run;
+        run += cnts[q];
+      }
+      if (lane == 31) S.cellPre[ncg] = incl;
+    }
+    __syncthreads();
+    const int total = S.cellPre[ncg];
+    for (int v0 = 0; v0 < total; v0 += kAffThreads) {
+      if (nb + kAffThreads > kCap) {
+        processBatch();
+        if (aborted) return;
+      }
+      const int v = v0 + tid;
+      bool keep = false;
+      int atom = -1;
+      double4 a = make_double4(0, 0, 0, 0);
+      if (v < total) {
+        int lo_i = 0, hi_i = ncg - 1;  // last cell with cellPre <= v
+        while (lo_i < hi_i) {
+          const int mid = (lo_i + hi_i + 1) >> 1;
+          if (S.cellPre[mid] <= v) lo_i = mid; else hi_i = mid - 1;
+        }
+        atom = P.cellAtoms[S.cellBeg[lo_i] + (v - S.cellPre[lo_i])];
+        a = P.xyz[atom];
+        const double ddx = fmax(fmax(lo[0] - a.x, a.x - hi[0]), 0.0);
+        const double ddy = fmax(fmax(lo[1] - a.y, a.y - hi[1]), 0.0);
+        const double ddz = fmax(fmax(lo[2] - a.z, a.z - hi[2]), 0.0);
+        keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.001;
+      }
+      const unsigned kbal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) S.cnt[warp] = __popc(kbal);
+      __syncthreads();
+      int tot = 0, off = 0;
+#pragma unroll
+      for (int w = 0; w < kAffThreads / 32; w++) {
+        if (w == warp) off = tot;
+        tot += S.cnt[w];
+      }
+      if (keep) {
+        const int j = nb + off + __popc(kbal & ((1u << lane) - 1u));
+        CandF& c = S.cand[j];
+        c.x = (float)(a.x - ox); c.y = (float)(a.y - oy); c.z = (float)(a.z - oz);
+        c.idx = atom;
+        c.vol = P.vol[atom];
+        c.solq = P.solq[atom];
+        c.info = P.info[atom];
+        c.rv[0] = P.rv[3 * atom]; c.rv[1] = P.rv[3 * atom + 1]; c.rv[2] = P.rv[3 * atom + 2];
+        c.rv2[0] = P.rv2[3 * atom]; c.rv2[1] = P.rv2[3 * atom + 1]; c.rv2[2] = P.rv2[3 * atom + 2];
+      }
+      nb += tot;
+      __syncthreads();
+    }
+  }
+  if (nb > 0) {
+    processBatch();
+    if (aborted) return;
   }
 
   if (!valid) return;
@@ -392,10 +450,10 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
     if (g >= P.nmaps) break;
     if (P.mapCov[g]) continue;
     float e = em[g] + (P.solparProbe[g] * S1 + P.volProbe[g] * S2);
-    const int slot = P.mapMinMaxSlot[g];
+    const int mslot = P.mapMinMaxSlot[g];
 #pragma unroll
     for (int s = 0; s < kMaxMinMax; s++)
-      if (s == slot && (mmFlag & (1u << s))) e += mn[s] + mx[s];
+      if (s == mslot && (mmFlag & (1u << s))) e += mn[s] + mx[s];
     P.out[(int64_t)g * P.npoints + pt] = e;
   }
   P.dmap[pt] = P.solparQ * S1;
@@ -418,171 +476,6 @@ cudaError_t aff_launch(const AffParams& P, cudaStream_t st) {
   else if (P.nmaps <= 12) AG_AFF(12);
   else AG_AFF(16);
 #undef AG_AFF
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Cell list: counting sort into 8 A cells; file order inside each cell.
-// ---------------------------------------------------------------------------
-__global__ void cell_count_kernel(CellBuild C) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C.n_atoms; i += gridDim.x * blockDim.x) {
-    int cell = -1;
-    if (!C.donorMask || C.donorMask[i]) {
-      const double4 a = C.xyz[i];
-      const int cx = (int)floor((a.x - C.lo[0]) / 8.0), cy = (int)floor((a.y - C.lo[1]) / 8.0),
-                cz = (int)floor((a.z - C.lo[2]) / 8.0);
-      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < C.ncell[0] && cy < C.ncell[1] && cz < C.ncell[2])
-        cell = (cz * C.ncell[1] + cy) * C.ncell[0] + cx;
-    }
-    C.cellOf[i] = cell;
-    if (cell >= 0) atomicAdd(&C.count[cell], 1);
-  }
-}
-
-// Exclusive scan of the counts by one CTA (cells are at most a few hundred thousand).
-__global__ void cell_scan_kernel(const int* count, int n, int* start) {
-  __shared__ int part[1024];
-  const int tid = threadIdx.x;
-  const int per = (n + 1023) / 1024;
-  const int b = tid * per, e = min(n, b + per);
-  int s = 0;
-  for (int i = b; i < e; i++) s += count[i];
-  part[tid] = s;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    int v = tid >= off ? part[tid - off] : 0;
-    __syncthreads();
-    part[tid] += v;
-    __syncthreads();
-  }
-  int run = part[tid] - s;
-  for (int i = b; i < e; i++) { start[i] = run; run += count[i]; }
-  if (tid == 1023) start[n] = part[1023];
-}
-
-__global__ void cell_scatter_kernel(CellBuild C) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C.n_atoms; i += gridDim.x * blockDim.x) {
-    const int cell = C.cellOf[i];
-    if (cell >= 0) C.cellAtoms[C.cellStart[cell] + atomicAdd(&C.fill[cell], 1)] = i;
-  }
-}
-
-// Restore file order inside each cell (one warp per cell, rank sort).
-__global__ void cell_sort_kernel(const int* cellStart, int ncell, int* cellAtoms, int* tmp) {
-  const int warpsPerBlock = blockDim.x / 32;
-  const int lane = threadIdx.x & 31;
-  for (int c = blockIdx.x * warpsPerBlock + threadIdx.x / 32; c < ncell; c += gridDim.x * warpsPerBlock) {
-    const int b = cellStart[c], e = cellStart[c + 1];
-    for (int i = b + lane; i < e; i += 32) {
-      const int v = cellAtoms[i];
-      int rank = 0;
-      for (int j = b; j < e; j++) rank += cellAtoms[j] < v;
-      tmp[b + rank] = v;
-    }
-    __syncwarp();
-    for (int i = b + lane; i < e; i += 32) cellAtoms[i] = tmp[i];
-  }
-}
-
-cudaError_t cells_launch(const CellBuild& C, int ncellTotal, cudaStream_t st) {
-  cudaMemsetAsync(C.count, 0, sizeof(int) * (ncellTotal + 1), st);
-  cudaMemsetAsync(C.fill, 0, sizeof(int) * (ncellTotal + 1), st);
-  const int blocks = max(1, min(1184, (C.n_atoms + 255) / 256));
-  cell_count_kernel<<<blocks, 256, 0, st>>>(C);
-  cell_scan_kernel<<<1, 1024, 0, st>>>(C.count, ncellTotal, C.cellStart);
-  cell_scatter_kernel<<<blocks, 256, 0, st>>>(C);
-  // cellOf (n_atoms entries) is free after the scatter and serves as the sort's scratch.
-  cell_sort_kernel<<<max(1, min(2048, (ncellTotal + 7) / 8)), 256, 0, st>>>(C.cellStart, ncellTotal, C.cellAtoms,
-                                                                         C.cellOf);
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Nearest H donor per grid point (argmin over DS/D1 atoms within the 27 cells
-// around the point's cell, ties to the lower file index), FP64 like the
-// reference's kd-tree query (CalculateGridmaps.cpp:246-250).
-// ---------------------------------------------------------------------------
-__global__ void closest_h_kernel(ClosestHParams P) {
-  for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < P.npoints;
-       pt += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(pt % P.nx), iy = (int)((pt / P.nx) % P.ny), iz = (int)(pt / ((int64_t)P.nx * P.ny));
-    const double gx = __dmul_rn((double)(ix - P.n2x), P.h), gy = __dmul_rn((double)(iy - P.n2y), P.h),
-                 gz = __dmul_rn((double)(iz - P.n2z), P.h);
-    const int cx = (int)floor((gx - P.cellLo[0]) / 8.0), cy = (int)floor((gy - P.cellLo[1]) / 8.0),
-              cz = (int)floor((gz - P.cellLo[2]) / 8.0);
-    int best = -1;
-    double bestR = 1e300;
-    for (int dz = -1; dz <= 1; dz++)
-      for (int dy = -1; dy <= 1; dy++)
-        for (int dx = -1; dx <= 1; dx++) {
-          const int x = cx + dx, y = cy + dy, z = cz + dz;
-          if (x < 0 || y < 0 || z < 0 || x >= P.ncell[0] || y >= P.ncell[1] || z >= P.ncell[2]) continue;
-          const int c = (z * P.ncell[1] + y) * P.ncell[0] + x;
-          for (int j = P.cellStart[c]; j < P.cellStart[c + 1]; j++) {
-            const int ia = P.cellAtoms[j];
-            const double4 a = P.xyz[ia];
-            const double r = rsq_exact(a.x, a.y, a.z, gx, gy, gz);
-            if (r < bestR || (r == bestR && ia < best)) { bestR = r; best = ia; }
-          }
-        }
-    P.closestH[pt] = (bestR <= 64.0) ? best : -1;
-  }
-}
-
-cudaError_t closest_h_launch(const ClosestHParams& P, cudaStream_t st) {
-  const int64_t blocks = (P.npoints + 255) / 256;
-  closest_h_kernel<<<(int)(blocks < 65535 * 16 ? blocks : 65535 * 16), 256, 0, st>>>(P);
-  return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
-// Covalent map and floating grid
-// ---------------------------------------------------------------------------
-__global__ void covalent_kernel(float* out, int nx, int ny, int nz, double h, double cx, double cy, double cz,
-                                double hwInv, double barrier) {
-  const int64_t n = (int64_t)nx * ny * nz;
-  for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < n; pt += (int64_t)gridDim.x * blockDim.x) {
-    const int ix = (int)(pt % nx), iy = (int)((pt / nx) % ny), iz = (int)(pt / ((int64_t)nx * ny));
-    const double dx = cx - __dmul_rn((double)(ix - nx / 2), h), dy = cy - __dmul_rn((double)(iy - ny / 2), h),
-                 dz = cz - __dmul_rn((double)(iz - nz / 2), h);
-    double r = __dmul_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)), hwInv);
-    if (r < 1.0e-12) r = 1.0e-12;
-    out[pt] = (float)(barrier * (1 - exp(-0.69314718055994529 * r)));
-  }
-}
-
-cudaError_t covalent_launch(float* out, int nx, int ny, int nz, double h, const double cov[3], double hwInv,
-                            double barrier, cudaStream_t st) {
-  covalent_kernel<<<1184, 256, 0, st>>>(out, nx, ny, nz, h, cov[0], cov[1], cov[2], hwInv, barrier);
-  return cudaGetLastError();
-}
-
-__global__ void floating_kernel(const double4* xyz, int n, int nx, int ny, int nz, double h, float* out) {
-  __shared__ double4 tile[256];
-  const int64_t np = (int64_t)nx * ny * nz;
-  const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool valid = pt < np;
-  const int ix = (int)(pt % nx), iy = (int)((pt / nx) % ny), iz = (int)(pt / ((int64_t)nx * ny));
-  const double gx = (double)(ix - nx / 2) * h, gy = (double)(iy - ny / 2) * h, gz = (double)(iz - nz / 2) * h;
-  double best = 1e24;
-  for (int t0 = 0; t0 < n; t0 += 256) {
-    if (t0 + (int)threadIdx.x < n) tile[threadIdx.x] = xyz[t0 + threadIdx.x];
-    __syncthreads();
-    const int m = min(256, n - t0);
-    for (int j = 0; j < m; j++) {
-      const double dx = tile[j].x - gx, dy = tile[j].y - gy, dz = tile[j].z - gz;
-      const double r = dx * dx + dy * dy + dz * dz;
-      best = r < best ? r : best;
-    }
-    __syncthreads();
-  }
-  if (valid) out[pt] = (float)sqrt(best);
-}
-
-cudaError_t floating_launch(const double4* xyz, int n, int nx, int ny, int nz, double h, float* out,
-                            cudaStream_t st) {
-  const int64_t np = (int64_t)nx * ny * nz;
-  floating_kernel<<<(int)((np + 255) / 256), 256, 0, st>>>(xyz, n, nx, ny, nz, h, out);
   return cudaGetLastError();
 }
 

@@ -34,6 +34,9 @@ struct EmapParams {
   const double* thr;              // thr[k]: least r^2 whose reference bin is >= k
   float rnear2;                   // (100 * rNear)^2
   float delta;                    // guard half-width around bin edges (units of 0.01 A)
+  int anaEvery;                   // every anaEvery-th mid atom of a tile takes the analytic path (0: none)
+  float negLambda2;               // -0.3153767175 / 100 / ln 2: E = 2^(negLambda2 * bin)
+  float poly[6];                  // invEps(bin) = sum_n poly[n] E^n for E <= 0.0121
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1
   unsigned* status;

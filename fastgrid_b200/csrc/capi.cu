@@ -161,6 +161,7 @@ struct ag_ctx {
   int emapMode = agk::kEmapKahan;
   float rNear = 14.0f;
   float delta = 2.0e-3f;
+  int anaEvery = 4;  // every 4th mid-list atom uses the analytic dielectric (0 = table only)
   int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
 };
 
@@ -339,6 +340,20 @@ int runEmap(ag_ctx* c, float* dOut) {
   P.thr = c->thr.p;
   P.rnear2 = (100.f * c->rNear) * (100.f * c->rNear);
   P.delta = c->delta;
+  // Series of 332/eps in E = exp(-0.3153767175 r): 332 (1 + a E) / (78.4 - c E)
+  // = (332 / 78.4) (1 + a E) sum_n (c / 78.4)^n E^n.
+  {
+    const double a = 7.7839, rho = 66.57180475 / 78.4, g0 = 332.0 / 78.4;
+    double rp = 1.0;
+    P.poly[0] = (float)g0;
+    for (int n = 1; n < 6; n++) {
+      const double prev = rp;
+      rp *= rho;
+      P.poly[n] = (float)(g0 * (rp + a * prev));
+    }
+    P.negLambda2 = (float)(-0.3153767175 / 100.0 / std::log(2.0));
+    P.anaEvery = c->anaEvery;
+  }
   P.out = dOut;
   P.status = c->status.p;
   // Split atoms across CTAs when the grid alone cannot fill the GPU.

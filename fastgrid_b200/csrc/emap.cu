@@ -48,10 +48,11 @@ struct EmapSmem {
   float tab[kTabLen];             // 32 KB
   double4 ring[2][kTile];         // 16 KB, TMA destination
   float4 nearA[kTile];            // local scaled x, y, z and 100*w
-  float4 midA[kTile];
+  float4 midA[kTile];             // mid atoms, table read
+  float4 midB[kTile];             // mid atoms, analytic bin value
   float4 farA[kTile];             // w pre-multiplied by invEps[8191]
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
-  int cnt[3][kThreads / 32];
+  int cnt[4][kThreads / 32];
   uint64_t bar[2];
 };
 
@@ -74,12 +75,35 @@ __device__ __forceinline__ void add_chunk(float (&sum)[kNX], float (&cmp)[kNX], 
   }
 }
 
-// Mid-list atoms: bin by a round-down FMA, table read, plain FP32 chunk sums.
+// Table read at the bin encoded in the low bits of f = 2^23 + bin: the shared
+// address is tabBiased + 4 * bits(f) in 32-bit shared-window arithmetic,
+// where tabBiased = address(tab) - 4 * bits(2^23) (mod 2^32).
+__device__ __forceinline__ float lds_bin(uint32_t tabBiased, float f) {
+  const uint32_t a = tabBiased + ((uint32_t)__float_as_int(f) << 2);
+  float v;
+  asm("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Mid-list atoms: bin by a round-down FMA, plain FP32 chunk sums.
+// ANALYTIC = false: the bin's value is read from the shared-memory table.
+// ANALYTIC = true: the same value is evaluated on the FMA and SFU pipes,
+//   invEps(bin) = 332 (1 + a E) / (78.4 - c E),  E = exp(-0.3153767175 bin / 100)
+//   (autogrid.h:233-239), as the series sum_n P.poly[n] E^n; mid atoms are
+//   at least 14 A away, so E <= 0.0121 and the truncation is below 1e-8
+//   relative.  Running part of the atoms this way takes load off the
+//   shared-memory pipe, whose random-bank table reads limit the kernel.
 // CLAMP: the CTA's box is large enough that a bin can pass the table's end.
-template <int MODE, bool CLAMP>
-__device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, const float* __restrict__ tab, int n,
+template <int MODE, bool CLAMP, bool ANALYTIC>
+__device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint32_t tabBiased, int n,
                                           const float (&gx)[kNX], float gy, float gz, float (&sum)[kNX],
-                                          float (&cmp)[kNX]) {
+                                          float (&cmp)[kNX], const EmapParams& P) {
   const float kBias = 8388608.f;
 #pragma unroll 1
   for (int j0 = 0; j0 < n; j0 += kChunk) {
@@ -99,7 +123,15 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, const
         const float rs = rsqrt_approx(r2);
         float f = __fmaf_rd(r2, rs, kBias);
         if (CLAMP) f = fminf(f, kBias + (float)(kTabLen - 1));
-        cs[k] = fmaf(a.w * rs, tab[__float_as_int(f) - 0x4B000000], cs[k]);
+        float g;
+        if (ANALYTIC) {
+          const float E = ex2_approx((f - kBias) * P.negLambda2);
+          g = fmaf(E, fmaf(E, fmaf(E, fmaf(E, fmaf(E, P.poly[5], P.poly[4]), P.poly[3]), P.poly[2]), P.poly[1]),
+                   P.poly[0]);
+        } else {
+          g = lds_bin(tabBiased, f);
+        }
+        cs[k] = fmaf(a.w * rs, g, cs[k]);
       }
     }
     if (MODE == kEmapKahan) {
@@ -195,20 +227,28 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
                   dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
       const float d2 = dx * dx + dy * dy + dz * dz;
       cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? 1 : 2);
+      if (cls == 1 && P.anaEvery > 0 && tid % P.anaEvery == P.anaEvery - 1) cls = 3;
       if (cls == 2) loc.w *= gFar;
     }
     const unsigned b0 = __ballot_sync(0xffffffffu, cls == 0);
     const unsigned b1 = __ballot_sync(0xffffffffu, cls == 1);
     const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-    if (lane == 0) { S.cnt[0][warp] = __popc(b0); S.cnt[1][warp] = __popc(b1); S.cnt[2][warp] = __popc(b2); }
+    const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
+    if (lane == 0) {
+      S.cnt[0][warp] = __popc(b0);
+      S.cnt[1][warp] = __popc(b1);
+      S.cnt[2][warp] = __popc(b2);
+      S.cnt[3][warp] = __popc(b3);
+    }
     __syncthreads();
-    int nNear = 0, nMid = 0, nFar = 0, off0 = 0, off1 = 0, off2 = 0;
+    int nNear = 0, nMid = 0, nFar = 0, nMidB = 0, off0 = 0, off1 = 0, off2 = 0, off3 = 0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) {
-      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; }
+      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; off3 = nMidB; }
       nNear += S.cnt[0][w];
       nMid += S.cnt[1][w];
       nFar += S.cnt[2][w];
+      nMidB += S.cnt[3][w];
     }
     const unsigned lt = (1u << lane) - 1u;
     if (cls == 0) {
@@ -219,13 +259,21 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
       S.midA[off1 + __popc(b1 & lt)] = loc;
     } else if (cls == 2) {
       S.farA[off2 + __popc(b2 & lt)] = loc;
+    } else if (cls == 3) {
+      S.midB[off3 + __popc(b3 & lt)] = loc;
     }
     __syncthreads();
 
-    // Mid atoms: table read, plain FP32 within a chunk.
+    // Mid atoms: table read (list A) or analytic bin value (list B).
     if (DDD) {
-      if (B.clampMid) mid_atoms<MODE, true>(S.midA, S.tab, nMid, gx, gy, gz, sum, cmp);
-      else mid_atoms<MODE, false>(S.midA, S.tab, nMid, gx, gy, gz, sum, cmp);
+      const uint32_t tabBiased = smem_u32(S.tab) - 0x2C000000u;
+      if (B.clampMid) {
+        mid_atoms<MODE, true, false>(S.midA, tabBiased, nMid, gx, gy, gz, sum, cmp, P);
+        mid_atoms<MODE, true, true>(S.midB, tabBiased, nMidB, gx, gy, gz, sum, cmp, P);
+      } else {
+        mid_atoms<MODE, false, false>(S.midA, tabBiased, nMid, gx, gy, gz, sum, cmp, P);
+        mid_atoms<MODE, false, true>(S.midB, tabBiased, nMidB, gx, gy, gz, sum, cmp, P);
+      }
     }
 
     // Far atoms: saturated dielectric (or the constant dielectric), no table.
