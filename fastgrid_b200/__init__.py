@@ -70,7 +70,8 @@ class SynthParams(C.Structure):
 EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", "ag_ctx_launch_count",
            "ag_emap", "ag_emap_mode", "ag_affinity", "ag_upload", "ag_compute", "ag_device_maps", "ag_download",
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
-           "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks"]
+           "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks",
+           "ag_emap_noalloc"]
 
 _lib = None
 
@@ -114,6 +115,7 @@ def lib():
     L.ag_main.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
     L.ag_synth_write.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(SynthParams)]
     L.ag_measure_peaks.argtypes = [C.c_int, dp, dp]
+    L.ag_emap_noalloc.argtypes = [C.POINTER(Grid), C.c_int, vp, vp, vp, vp]
     _lib = L
     return L
 

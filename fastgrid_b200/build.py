@@ -17,7 +17,7 @@ OUT = os.path.join(HERE, "_lib")
 OBJ = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU = ["emap.cu", "affinity.cu", "cells.cu", "capi.cu", "peaks.cu"]
+CU = ["emap.cu", "affinity.cu", "cells.cu", "capi.cu", "peaks.cu", "emap_noalloc.cu"]
 CPP = ["host.cpp", "synth.cpp"]
 LIB = os.path.join(OUT, "libfastgrid_b200.so")
 

@@ -167,6 +167,11 @@ struct ag_ctx {
 
 extern "C" const char* ag_last_error(void) { return g_err.c_str(); }
 
+namespace ag {
+// Lets other translation units of the library report through ag_last_error().
+void setLastError(const char* msg) { g_err = msg; }
+}  // namespace ag
+
 extern "C" int ag_ctx_create(int device, ag_ctx** out) {
   if (!out) return fail(AG_E_INVALID, "null output pointer");
   int n = 0;
