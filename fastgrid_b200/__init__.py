@@ -25,6 +25,7 @@ CLI_PATH = os.path.join(HERE, "_lib", "fastgrid4")
 AG_OK = 0
 AG_WORK_EMAP, AG_WORK_AFFINITY, AG_WORK_ALL = 1, 2, 3
 AG_EMAP_KAHAN, AG_EMAP_PLAIN = 0, 1
+AG_TUNE_EMAP_RNEAR, AG_TUNE_EMAP_ANALYTIC_EVERY, AG_TUNE_EMAP_CTAS_PER_SM = 1, 2, 3
 TABLE_LEN = 8192
 
 
@@ -71,7 +72,7 @@ EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", 
            "ag_emap", "ag_emap_mode", "ag_affinity", "ag_upload", "ag_compute", "ag_device_maps", "ag_download",
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
            "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks",
-           "ag_emap_noalloc"]
+           "ag_emap_noalloc", "ag_ctx_tune"]
 
 _lib = None
 
@@ -116,6 +117,7 @@ def lib():
     L.ag_synth_write.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(SynthParams)]
     L.ag_measure_peaks.argtypes = [C.c_int, dp, dp]
     L.ag_emap_noalloc.argtypes = [C.POINTER(Grid), C.c_int, vp, vp, vp, vp]
+    L.ag_ctx_tune.argtypes = [vp, C.c_int, C.c_double]
     _lib = L
     return L
 
@@ -155,6 +157,9 @@ class Context:
     @property
     def stream(self):
         return lib().ag_ctx_stream(self.h)
+
+    def tune(self, knob, value):
+        _check(lib().ag_ctx_tune(self.h, knob, float(value)))
 
     @property
     def launches(self):

@@ -314,6 +314,18 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
           S1 = fmaf(sv, a.vol, S1);
           S2 = fmaf(sv, a.solq, S2);
           const float4* row4 = reinterpret_cast<const float4*>(tab + iR * nmPad);
+          if (modes == 0u) {  // no H-bond terms for this receptor type (uniform): plain sums
+#pragma unroll
+            for (int g4 = 0; g4 < NMAX / 4; g4++) {
+              if (4 * g4 >= P.nmaps) break;
+              const float4 q = row4[g4];
+              em[4 * g4] += q.x;
+              em[4 * g4 + 1] += q.y;
+              em[4 * g4 + 2] += q.z;
+              em[4 * g4 + 3] += q.w;
+            }
+            continue;
+          }
           float4 q4 = make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
           for (int g = 0; g < NMAX; g++) {

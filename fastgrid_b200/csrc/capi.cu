@@ -161,7 +161,8 @@ struct ag_ctx {
   int emapMode = agk::kEmapKahan;
   float rNear = 14.0f;
   float delta = 2.0e-3f;
-  int anaEvery = 4;  // every 4th mid-list atom uses the analytic dielectric (0 = table only)
+  int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
+  int ctasPerSm = 2;
   int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
 };
 
@@ -218,6 +219,26 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return AG_OK;
+}
+
+extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
+  if (!c) return fail(AG_E_INVALID, "null context");
+  switch (knob) {
+    case AG_TUNE_EMAP_RNEAR:
+      if (!(v >= 8.0 && v <= 40.0)) return fail(AG_E_INVALID, "rNear must be in [8, 40] A");
+      c->rNear = (float)v;
+      return AG_OK;
+    case AG_TUNE_EMAP_ANALYTIC_EVERY:
+      if (!(v == 0.0 || (v >= 2.0 && v <= 64.0))) return fail(AG_E_INVALID, "analytic-every must be 0 or 2..64");
+      c->anaEvery = (int)v;
+      return AG_OK;
+    case AG_TUNE_EMAP_CTAS_PER_SM:
+      if (!(v >= 1.0 && v <= 8.0)) return fail(AG_E_INVALID, "CTAs per SM must be 1..8");
+      c->ctasPerSm = (int)v;
+      return AG_OK;
+    default:
+      return fail(AG_E_INVALID, "unknown tuning knob %d", knob);
+  }
 }
 
 extern "C" void* ag_ctx_stream(ag_ctx* c) { return c ? (void*)c->stream : nullptr; }
@@ -364,7 +385,7 @@ int runEmap(ag_ctx* c, float* dOut) {
   // Split atoms across CTAs when the grid alone cannot fill the GPU.
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-  const int want = 2 * sms * 2;
+  const int want = 2 * sms * c->ctasPerSm;  // two waves of resident CTAs
   int nsplit = 1;
   if (P.nblocks < want && c->nAtoms > 512) nsplit = std::min((want + P.nblocks - 1) / P.nblocks, (c->nAtoms + 255) / 256);
   int chunk = (c->nAtoms + nsplit - 1) / nsplit;

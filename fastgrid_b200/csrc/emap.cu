@@ -307,8 +307,8 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
       const float dy = a.y - gy, dz = a.z - gz;
       const float dyz2 = fmaf(dz, dz, dy * dy);
       float rsv[kNX];
+      float fT[kNX];  // 100 r (FP32), kept for the rare exact-bin fallback
       int idx[kNX];
-      int kmid[kNX];
       unsigned flags = 0;
 #pragma unroll
       for (int k = 0; k < kNX; k++) {
@@ -318,12 +318,13 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
         rsv[k] = rs;
         if (DDD) {
           const float T = r2 * rs;
+          fT[k] = T;
           float f = __fmaf_rd(r2, rs, kBias);
           f = fminf(f, kBias + (float)(kTabLen - 1));
           idx[k] = __float_as_int(f) - 0x4B000000;
-          const float kr = (T + 12582912.f) - 12582912.f;  // nearest integer (T < 2^22)
-          kmid[k] = (int)kr;
-          if (fabsf(T - kr) < P.delta && kr >= 1.f && kr < (float)kTabLen) flags |= 1u << k;
+          // Within delta of a bin edge <=> the fraction of T is within delta of 0 or 1.
+          const float fr = T - (f - kBias);
+          if (fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
         }
       }
       if (DDD && __any_sync(0xffffffffu, flags != 0)) {
@@ -335,10 +336,12 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
 #pragma unroll
           for (int k = 0; k < kNX; k++) {
             if (flags & (1u << k)) {
+              // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
+              const int kmid = min(__float_as_int(fT[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
               const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
               const double ddx = __dsub_rn(a64.x, gx64);
               const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
-              idx[k] = (r2d >= P.thr[kmid[k]]) ? kmid[k] : kmid[k] - 1;
+              idx[k] = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
             }
           }
         }

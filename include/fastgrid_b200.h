@@ -87,6 +87,14 @@ void* ag_ctx_stream(ag_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t ag_ctx_launch_count(const ag_ctx* ctx);
 
+/* Tuning knobs of a context (no reference counterpart; the reference's
+ * --cuda-* switches played this role for its kernels).  Results stay within
+ * the stated tolerances for every allowed value. */
+#define AG_TUNE_EMAP_RNEAR 1          /* A, >= 8: atoms nearer the CTA box take the exact-bin path (default 14) */
+#define AG_TUNE_EMAP_ANALYTIC_EVERY 2 /* 0 or >= 2: every n-th mid atom evaluates 332/eps analytically (default 0) */
+#define AG_TUNE_EMAP_CTAS_PER_SM 3    /* 1..8: CTAs per SM the atom split aims for on small grids (default 2) */
+int ag_ctx_tune(ag_ctx* ctx, int knob, double value);
+
 /* ------------------------------------------------------------------------ */
 /* Electrostatic map.                                                        */
 /* Replaces calculateElectrostaticMapAsync + synchronizeCalculation          */
