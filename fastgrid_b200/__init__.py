@@ -72,7 +72,8 @@ EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", 
            "ag_emap", "ag_emap_mode", "ag_affinity", "ag_upload", "ag_compute", "ag_device_maps", "ag_download",
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
            "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks",
-           "ag_emap_noalloc", "ag_ctx_tune"]
+           "ag_emap_noalloc", "ag_ctx_tune", "ag_batch_create", "ag_batch_autotune",
+           "ag_batch_compute", "ag_batch_download", "ag_batch_pairs", "ag_batch_free"]
 
 _lib = None
 
@@ -118,6 +119,13 @@ def lib():
     L.ag_measure_peaks.argtypes = [C.c_int, dp, dp]
     L.ag_emap_noalloc.argtypes = [C.POINTER(Grid), C.c_int, vp, vp, vp, vp]
     L.ag_ctx_tune.argtypes = [vp, C.c_int, C.c_double]
+    L.ag_batch_create.argtypes = [vp, C.POINTER(vp), C.c_int, C.POINTER(vp)]
+    L.ag_batch_autotune.argtypes = [vp, C.c_char_p]
+    L.ag_batch_compute.argtypes = [vp]
+    L.ag_batch_download.argtypes = [vp, C.c_int, fp]
+    L.ag_batch_pairs.argtypes = [vp]
+    L.ag_batch_pairs.restype = C.c_double
+    L.ag_batch_free.argtypes = [vp]
     _lib = L
     return L
 
@@ -256,6 +264,44 @@ def measure_peaks(device=0):
     a, b = C.c_double(), C.c_double()
     _check(lib().ag_measure_peaks(device, C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+class Batch:
+    """Many map sets computed by persistent kernels replayed from one CUDA graph."""
+
+    def __init__(self, ctx, problems):
+        self.problems = list(problems)  # keep the problems alive
+        arr = (C.c_void_p * len(self.problems))(*[p.h.value for p in self.problems])
+        h = C.c_void_p()
+        _check(lib().ag_batch_create(ctx.h, arr, len(self.problems), C.byref(h)))
+        self.h = h
+
+    def autotune(self, cache_path=None):
+        _check(lib().ag_batch_autotune(self.h, cache_path.encode() if cache_path else None))
+
+    def compute(self):
+        _check(lib().ag_batch_compute(self.h))
+
+    @property
+    def pairs(self):
+        return lib().ag_batch_pairs(self.h)
+
+    def maps(self, i):
+        p = self.problems[i]
+        out = np.empty((p.n_maps + 2) * p.npoints, dtype=np.float32)
+        _check(lib().ag_batch_download(self.h, i, _fp(out)))
+        return out.reshape(p.n_maps + 2, p.grid.nz, p.grid.ny, p.grid.nx)
+
+    def close(self):
+        if self.h:
+            lib().ag_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def main(argv):

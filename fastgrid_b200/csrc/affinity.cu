@@ -92,9 +92,10 @@ __device__ double costheta_exact(double ax, double ay, double az, double gx, dou
   return -__dadd_rn(__dadd_rn(__dmul_rn(ux, rv[0]), __dmul_rn(uy, rv[1])), __dmul_rn(uz, rv[2]));
 }
 
+// One work unit: the CTA block `cta` of job P.  Called once per CTA by
+// affinity_kernel and repeatedly by the persistent batch kernel.
 template <int NMAX>
-__global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+__device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsigned char* smem_raw) {
   AffSmem& S = *reinterpret_cast<AffSmem*>(smem_raw);
   float* tabBuf = reinterpret_cast<float*>(smem_raw + ((sizeof(AffSmem) + 127) / 128) * 128);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -104,7 +105,7 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
 
   // This CTA's block of points and this thread's point.
   const int tbx = (P.nx + kAffTX - 1) / kAffTX, tby = (P.ny + kAffTY - 1) / kAffTY;
-  const int bx = blockIdx.x % tbx, by = (blockIdx.x / tbx) % tby, bz = blockIdx.x / (tbx * tby);
+  const int bx = cta % tbx, by = (cta / tbx) % tby, bz = cta / (tbx * tby);
   const int x0 = bx * kAffTX, y0 = by * kAffTY, z0 = bz * kAffTZ;
   const int ix = x0 + (tid % kAffTX), iy = y0 + (tid / kAffTX) % kAffTY, iz = z0 + tid / (kAffTX * kAffTY);
   const bool valid = ix < P.nx && iy < P.ny && iz < P.nz;
@@ -469,6 +470,50 @@ __global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(AffParams P) {
     P.out[(int64_t)g * P.npoints + pt] = e;
   }
   P.dmap[pt] = P.solparQ * S1;
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kAffThreads, 2) affinity_kernel(const __grid_constant__ AffParams P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  aff_unit<NMAX>(P, blockIdx.x, smem_raw);
+}
+
+// Persistent kernel over the work units (job, CTA block) of a batch of
+// receptors, taken from an atomic counter in the host's (decreasing cost) order.
+template <int NMAX>
+__global__ void __launch_bounds__(kAffThreads, 2)
+    affinity_batch_kernel(const AffParams* __restrict__ jobs, const int2* __restrict__ units, int nunits,
+                          int* counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int s_unit;
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_unit = atomicAdd(counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    if (u >= nunits) return;
+    const int2 w = units[u];
+    aff_unit<NMAX>(jobs[w.x], w.y, smem_raw);
+  }
+}
+
+cudaError_t aff_batch_launch(const AffParams* jobs, const int2* units, int nunits, int* counter, int nmPadMax,
+                             int nmapsMax, int grid, cudaStream_t st) {
+  const size_t smem = aff_smem_bytes(nmPadMax);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+#define AG_AFFB(N)                                                                                               \
+  do {                                                                                                           \
+    e = cudaFuncSetAttribute(affinity_batch_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (e != cudaSuccess) return e;                                                                              \
+    affinity_batch_kernel<N><<<grid, kAffThreads, smem, st>>>(jobs, units, nunits, counter);                     \
+  } while (0)
+  if (nmapsMax <= 4) AG_AFFB(4);
+  else if (nmapsMax <= 8) AG_AFFB(8);
+  else if (nmapsMax <= 12) AG_AFFB(12);
+  else AG_AFFB(16);
+#undef AG_AFFB
+  return cudaGetLastError();
 }
 
 cudaError_t aff_launch(const AffParams& P, cudaStream_t st) {

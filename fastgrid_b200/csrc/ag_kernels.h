@@ -40,10 +40,14 @@ struct EmapParams {
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1
   unsigned* status;
+  double* checksum;               // per split: FP64 sum of the weights the split's first CTA consumed (or null)
 };
 
 cudaError_t emap_launch(const EmapParams& P, bool ddd, int mode, int grid, cudaStream_t st);
 size_t emap_smem_bytes();
+// Persistent e-map over the units (job, CTA box) of many jobs (no atom split, distance-dependent dielectric).
+cudaError_t emap_batch_launch(const EmapParams* jobs, const int2* units, int nunits, int* counter, int grid,
+                              cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // Affinity + desolvation
@@ -99,6 +103,9 @@ struct AffParams {
 
 size_t aff_smem_bytes(int nmPad);
 cudaError_t aff_launch(const AffParams& P, cudaStream_t st);
+// Persistent affinity pass over the units (job, CTA block) of many jobs.
+cudaError_t aff_batch_launch(const AffParams* jobs, const int2* units, int nunits, int* counter, int nmPadMax,
+                             int nmapsMax, int grid, cudaStream_t st);
 
 // Cell list build (counting sort of atoms into 8 A cells, file order kept inside each cell).
 struct CellBuild {

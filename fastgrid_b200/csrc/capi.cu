@@ -138,6 +138,8 @@ struct ag_ctx {
   std::vector<agk::EmapBlock> hBlocks;
   int itemsFor[3] = {0, 0, 0};
   double itemsH = 0;
+  int itemsTile = 0;
+  int tile[3] = {2, 16, 8};  // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
   // affinity
   DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
   DevBuf<float> vol, solq, affTab, affTabH, sol, rv32, rv2_32;
@@ -163,6 +165,9 @@ struct ag_ctx {
   float delta = 2.0e-3f;
   int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
   int ctasPerSm = 2;
+  DevBuf<double> checksum;
+  int checksumSplits = 0;
+  double wSum = 0, wAbsSum = 0, lastChecksum = 0;
   int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
 };
 
@@ -211,6 +216,7 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   c->partial.release();
   c->rv64.release();
   c->thrA.release();
+  c->checksum.release();
   c->blocks.release();
   c->status.release();
   for (auto* b : {&c->items, &c->info, &c->cellStart, &c->cellAtoms, &c->cellOf, &c->count, &c->fill, &c->dStart,
@@ -261,9 +267,11 @@ int checkGrid(const ag_grid* g) {
 // 256 items walking 2 x 16 x 8 tiles of items, with each CTA's box.
 void buildItems(ag_ctx* c) {
   const ag_grid& g = c->grid;
-  if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing) return;
+  if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing &&
+      c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2])
+    return;
   const int nxc = (g.nx + agk::kNX - 1) / agk::kNX;
-  const int TX = 2, TY = 16, TZ = 8;
+  const int TX = c->tile[0], TY = c->tile[1], TZ = c->tile[2];
   c->hItems.clear();
   // Tiles in boustrophedon order (y rows and x columns reverse direction on
   // alternate passes), so a CTA that continues from one tile into the next
@@ -318,6 +326,7 @@ void buildItems(ag_ctx* c) {
   c->itemsFor[1] = g.ny;
   c->itemsFor[2] = g.nz;
   c->itemsH = g.spacing;
+  c->itemsTile = c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2];
 }
 
 int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, bool deviceInputs) {
@@ -330,6 +339,12 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
   if (!deviceInputs) {
     for (int64_t i = 0; i < 4 * (int64_t)n; i++)
       if (!std::isfinite(xyzw[i])) return fail(AG_E_INVALID, "non-finite atom coordinate or weight at atom %lld", (long long)(i / 4));
+    c->wSum = 0;
+    c->wAbsSum = 0;
+    for (int i = 0; i < n; i++) {
+      c->wSum += xyzw[4 * (size_t)i + 3];
+      c->wAbsSum += std::fabs(xyzw[4 * (size_t)i + 3]);
+    }
     CK(c->atoms.ensure(n));
     if (n) CK(cudaMemcpyAsync(c->atoms.p, xyzw, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream));
   }
@@ -350,9 +365,11 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
   return AG_OK;
 }
 
-int runEmap(ag_ctx* c, float* dOut) {
+// Launch parameters of the e-map of the staged job; allowSplit = false keeps
+// every CTA on all atoms (the batch kernel's mode).
+int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P) {
   const int64_t np = c->npoints();
-  agk::EmapParams P{};
+  P = agk::EmapParams{};
   P.atoms = c->atoms.p;
   P.n_atoms = c->nAtoms;
   P.nblocks = (int)c->hBlocks.size();
@@ -387,7 +404,8 @@ int runEmap(ag_ctx* c, float* dOut) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
   const int want = 2 * sms * c->ctasPerSm;  // two waves of resident CTAs
   int nsplit = 1;
-  if (P.nblocks < want && c->nAtoms > 512) nsplit = std::min((want + P.nblocks - 1) / P.nblocks, (c->nAtoms + 255) / 256);
+  if (allowSplit && P.nblocks < want && c->nAtoms > 512)
+    nsplit = std::min((want + P.nblocks - 1) / P.nblocks, (c->nAtoms + 255) / 256);
   int chunk = (c->nAtoms + nsplit - 1) / nsplit;
   chunk = ((chunk + 255) / 256) * 256;
   if (chunk == 0) chunk = 256;
@@ -398,10 +416,21 @@ int runEmap(ag_ctx* c, float* dOut) {
     CK(c->partial.ensure((size_t)nsplit * np));
     P.partial = c->partial.p;
   }
+  return AG_OK;
+}
+
+int runEmap(ag_ctx* c, float* dOut) {
+  const int64_t np = c->npoints();
+  agk::EmapParams P;
+  if (int e = buildEmapParams(c, dOut, true, P)) return e;
+  const int nsplit = P.nsplit;
   if (c->nAtoms == 0) {
     CK(cudaMemsetAsync(dOut, 0, sizeof(float) * np, c->stream));
     return AG_OK;
   }
+  CK(c->checksum.ensure(nsplit));
+  P.checksum = c->checksum.p;
+  c->checksumSplits = nsplit;
   CK(agk::emap_launch(P, c->ddd, c->emapMode, P.nblocks * nsplit, c->stream));
   c->launches += nsplit > 1 ? 2 : 1;
   return AG_OK;
@@ -527,20 +556,26 @@ int stageAffinity(ag_ctx* c, const ag_receptor* r, const ag_affinity_params* p) 
   return AG_OK;
 }
 
-int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
+// 8 A cells over the grid box widened by 8 A (atoms further out cannot reach a point).
+void cellGrid(const ag_grid& g, double lo[3], int ncell[3]) {
+  const double h = g.spacing;
+  const int nn[3] = {g.nx, g.ny, g.nz};
+  for (int d = 0; d < 3; d++) {
+    lo[d] = (double)(0 - nn[d] / 2) * h - 8.0;
+    const double hi = (double)(nn[d] - 1 - nn[d] / 2) * h + 8.0;
+    ncell[d] = std::max(1, (int)std::ceil((hi - lo[d]) / 8.0));
+  }
+}
+
+// Cell lists (all atoms, H donors) and the nearest donor of every point, on stream st.
+int prepAffinity(ag_ctx* c, cudaStream_t st) {
   const ag_grid& g = c->grid;
   const int64_t np = c->npoints();
   const int n = c->nAtoms;
   const double h = g.spacing;
-  // 8 A cells over the grid box widened by 8 A (atoms further out cannot reach a point).
-  double lo[3], hi[3];
-  const int nn[3] = {g.nx, g.ny, g.nz};
+  double lo[3];
   int ncell[3];
-  for (int d = 0; d < 3; d++) {
-    lo[d] = (double)(0 - nn[d] / 2) * h - 8.0;
-    hi[d] = (double)(nn[d] - 1 - nn[d] / 2) * h + 8.0;
-    ncell[d] = std::max(1, (int)std::ceil((hi[d] - lo[d]) / 8.0));
-  }
+  cellGrid(g, lo, ncell);
   const int ncellT = ncell[0] * ncell[1] * ncell[2];
   CK(c->cellStart.ensure(ncellT + 1)); CK(c->count.ensure(ncellT + 1)); CK(c->fill.ensure(ncellT + 1));
   CK(c->cellAtoms.ensure(n)); CK(c->cellOf.ensure(n));
@@ -551,18 +586,30 @@ int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
   for (int d = 0; d < 3; d++) { C.lo[d] = lo[d]; C.ncell[d] = ncell[d]; }
   C.cellOf = c->cellOf.p; C.count = c->count.p; C.fill = c->fill.p;
   C.cellStart = c->cellStart.p; C.cellAtoms = c->cellAtoms.p; C.donorMask = nullptr;
-  CK(agk::cells_launch(C, ncellT, c->stream));
+  CK(agk::cells_launch(C, ncellT, st));
   C.cellStart = c->dStart.p; C.cellAtoms = c->dAtoms.p; C.donorMask = c->donorMask.p;
-  CK(agk::cells_launch(C, ncellT, c->stream));
+  CK(agk::cells_launch(C, ncellT, st));
   c->launches += 8;
   agk::ClosestHParams H{};
   H.xyz = c->atoms.p; H.cellStart = c->dStart.p; H.cellAtoms = c->dAtoms.p;
   for (int d = 0; d < 3; d++) { H.cellLo[d] = lo[d]; H.ncell[d] = ncell[d]; }
   H.nx = g.nx; H.ny = g.ny; H.nz = g.nz; H.n2x = g.nx / 2; H.n2y = g.ny / 2; H.n2z = g.nz / 2;
   H.npoints = np; H.h = h; H.closestH = c->closestH.p;
-  CK(agk::closest_h_launch(H, c->stream));
+  CK(agk::closest_h_launch(H, st));
   c->launches += 1;
+  return AG_OK;
+}
 
+// Launch parameters of the affinity passes of the staged job.
+int buildAffParams(ag_ctx* c, float* dMaps, float* dDmap, std::vector<agk::AffParams>& out) {
+  const ag_grid& g = c->grid;
+  const int64_t np = c->npoints();
+  const int n = c->nAtoms;
+  const double h = g.spacing;
+  double lo[3];
+  int ncell[3];
+  cellGrid(g, lo, ncell);
+  out.clear();
   const int nt = c->nTypes;
   std::vector<ag_ctx::Pass> passes = c->passes;
   if (passes.empty()) {  // no ligand maps: one pass for the d-map alone
@@ -601,6 +648,16 @@ int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
     P.out = dMaps + (size_t)ps.m0 * np;
     P.dmap = dDmap;
     P.status = c->status.p;
+    out.push_back(P);
+  }
+  return AG_OK;
+}
+
+int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
+  if (int e = prepAffinity(c, c->stream)) return e;
+  std::vector<agk::AffParams> passes;
+  if (int e = buildAffParams(c, dMaps, dDmap, passes)) return e;
+  for (const auto& P : passes) {
     CK(agk::aff_launch(P, c->stream));
     c->launches += 1;
   }
@@ -615,6 +672,19 @@ int checkStatus(ag_ctx* c) {
     cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), c->stream);
     cudaStreamSynchronize(c->stream);
     return fail(AG_E_DEVICE, "a kernel reported error status 0x%x (1 = bounded wait expired, 2 = bad input)", st);
+  }
+  // Net-charge checksum of the last e-map: the FP64 sum of the weights the
+  // kernel consumed must equal the host's sum of the input weights.
+  if (c->checksumSplits > 0) {
+    std::vector<double> cs(c->checksumSplits);
+    CK(cudaMemcpyAsync(cs.data(), c->checksum.p, sizeof(double) * cs.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    double s = 0.0;
+    for (double v : cs) s += v;
+    c->checksumSplits = 0;
+    c->lastChecksum = s;
+    if (!(std::fabs(s - c->wSum) <= 1e-9 * c->wAbsSum + 1e-12))
+      return fail(AG_E_DEVICE, "net-charge checksum mismatch: kernel summed %.17g, input holds %.17g", s, c->wSum);
   }
   return AG_OK;
 }
@@ -806,6 +876,263 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
 }
 
 extern "C" const float* ag_problem_maps(const ag_problem* P) { return P && !P->p.out.empty() ? P->p.out.data() : nullptr; }
+
+// ---------------------------------------------------------------------------
+// Batches: persistent kernels over the work units of many jobs, one CUDA graph
+// ---------------------------------------------------------------------------
+struct ag_batch {
+  ag_ctx* ctx = nullptr;                 // stream and device of the batch
+  std::vector<ag_ctx*> sub;              // per job: staged inputs and outputs
+  std::vector<ag_problem*> probs;
+  DevBuf<agk::EmapParams> ejobs;
+  DevBuf<int2> eunits;
+  DevBuf<agk::AffParams> ajobs;
+  DevBuf<int2> aunits;
+  DevBuf<int> counters;
+  int ne = 0, na = 0, nmPadMax = 4, nmapsMax = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double pairs = 0;
+};
+
+namespace {
+
+void batchDropGraph(ag_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+int restageItems(ag_ctx* c) {
+  buildItems(c);
+  CK(c->items.ensure(c->hItems.size()));
+  CK(c->blocks.ensure(c->hBlocks.size()));
+  CK(cudaMemcpy(c->items.p, c->hItems.data(), sizeof(int) * c->hItems.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->blocks.p, c->hBlocks.data(), sizeof(agk::EmapBlock) * c->hBlocks.size(), cudaMemcpyHostToDevice));
+  return AG_OK;
+}
+
+// Job parameters and work units (largest jobs first) for the current tile shapes.
+int batchBuild(ag_batch* b) {
+  batchDropGraph(b);
+  std::vector<agk::EmapParams> ej;
+  std::vector<agk::AffParams> aj;
+  std::vector<std::pair<double, int2>> eu, au;
+  b->nmPadMax = 4;
+  b->nmapsMax = 0;
+  b->pairs = 0;
+  for (size_t i = 0; i < b->sub.size(); i++) {
+    ag_ctx* c = b->sub[i];
+    const int64_t np = c->npoints();
+    agk::EmapParams P;
+    if (int e = buildEmapParams(c, c->maps.p + (size_t)c->nMaps * np, false, P)) return e;
+    P.checksum = nullptr;
+    const int j = (int)ej.size();
+    ej.push_back(P);
+    for (int k = 0; k < P.nblocks; k++)
+      eu.push_back({(double)c->nAtoms * c->hBlocks[k].nitems, make_int2(j, k)});
+    b->pairs += (double)c->nAtoms * (double)np;
+    std::vector<agk::AffParams> passes;
+    if (int e = buildAffParams(c, c->maps.p, c->maps.p + (size_t)(c->nMaps + 1) * np, passes)) return e;
+    const int ncta = ((c->grid.nx + agk::kAffTX - 1) / agk::kAffTX) * ((c->grid.ny + agk::kAffTY - 1) / agk::kAffTY) *
+                     ((c->grid.nz + agk::kAffTZ - 1) / agk::kAffTZ);
+    for (const auto& A : passes) {
+      const int ja = (int)aj.size();
+      aj.push_back(A);
+      b->nmPadMax = std::max(b->nmPadMax, A.nmPad);
+      b->nmapsMax = std::max(b->nmapsMax, A.nmaps);
+      for (int k = 0; k < ncta; k++) au.push_back({(double)c->nAtoms, make_int2(ja, k)});
+    }
+  }
+  auto byCost = [](const std::pair<double, int2>& x, const std::pair<double, int2>& y) {
+    return x.first > y.first || (x.first == y.first && (x.second.x < y.second.x ||
+                                                         (x.second.x == y.second.x && x.second.y < y.second.y)));
+  };
+  std::sort(eu.begin(), eu.end(), byCost);
+  std::sort(au.begin(), au.end(), byCost);
+  std::vector<int2> eul, aul;
+  for (auto& u : eu) eul.push_back(u.second);
+  for (auto& u : au) aul.push_back(u.second);
+  b->ne = (int)eul.size();
+  b->na = (int)aul.size();
+  CK(b->ejobs.ensure(ej.size()));
+  CK(b->ajobs.ensure(aj.size()));
+  CK(b->eunits.ensure(eul.size()));
+  CK(b->aunits.ensure(aul.size()));
+  CK(b->counters.ensure(2));
+  CK(cudaMemcpy(b->ejobs.p, ej.data(), sizeof(agk::EmapParams) * ej.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->ajobs.p, aj.data(), sizeof(agk::AffParams) * aj.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->eunits.p, eul.data(), sizeof(int2) * eul.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->aunits.p, aul.data(), sizeof(int2) * aul.size(), cudaMemcpyHostToDevice));
+  return AG_OK;
+}
+
+int batchSizeClass(const ag_ctx* c) {
+  const int a = c->nAtoms < 3000 ? 0 : (c->nAtoms < 10000 ? 1 : 2);
+  const int64_t np = const_cast<ag_ctx*>(c)->npoints();
+  const int g = np < 200000 ? 0 : (np < 1500000 ? 1 : 2);
+  return a * 3 + g;
+}
+
+}  // namespace
+
+extern "C" int ag_batch_create(ag_ctx* ctx, ag_problem* const* problems, int n, ag_batch** out) {
+  if (!ctx || !problems || n <= 0 || !out) return fail(AG_E_INVALID, "bad batch arguments");
+  auto* b = new ag_batch();
+  b->ctx = ctx;
+  for (int i = 0; i < n; i++) {
+    if (!problems[i] || !problems[i]->p.distDepDiel) {
+      ag_batch_free(b);
+      return fail(AG_E_INVALID, "batch job %d is missing or does not use the distance-dependent dielectric", i);
+    }
+    ag_ctx* c = nullptr;
+    if (int e = ag_ctx_create(ctx->device, &c)) { ag_batch_free(b); return e; }
+    b->sub.push_back(c);
+    b->probs.push_back(problems[i]);
+    ag_grid g;
+    ag_receptor r;
+    ag_affinity_params a;
+    const double* eps = nullptr;
+    ag_problem_views(problems[i], &g, &r, &a, &eps);
+    if (int e = ag_upload(c, &g, &r, &a, eps)) { ag_batch_free(b); return e; }
+    // Allocate every per-job buffer now (the graph capture must not allocate).
+    if (int e = prepAffinity(c, c->stream)) { ag_batch_free(b); return e; }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) { ag_batch_free(b); return fail(AG_E_CUDA, "staging failed"); }
+  }
+  if (int e = batchBuild(b)) { ag_batch_free(b); return e; }
+  *out = b;
+  return AG_OK;
+}
+
+extern "C" double ag_batch_pairs(const ag_batch* b) { return b ? b->pairs : 0.0; }
+
+extern "C" int ag_batch_compute(ag_batch* b) {
+  if (!b) return fail(AG_E_INVALID, "null batch");
+  cudaStream_t st = b->ctx->stream;
+  CK(cudaSetDevice(b->ctx->device));
+  if (!b->exec) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ctx->device);
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int err = AG_OK;
+    for (ag_ctx* c : b->sub)
+      if (!err) err = prepAffinity(c, st);
+    if (!err && agk::emap_batch_launch(b->ejobs.p, b->eunits.p, b->ne, b->counters.p, 2 * sms, st) != cudaSuccess)
+      err = fail(AG_E_CUDA, "batch e-map launch failed");
+    if (!err && agk::aff_batch_launch(b->ajobs.p, b->aunits.p, b->na, b->counters.p + 1, b->nmPadMax, b->nmapsMax,
+                                      2 * sms, st) != cudaSuccess)
+      err = fail(AG_E_CUDA, "batch affinity launch failed");
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (err) {
+      if (g) cudaGraphDestroy(g);
+      return err;
+    }
+    if (ce != cudaSuccess) return fail(AG_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  }
+  CK(cudaGraphLaunch(b->exec, st));
+  b->ctx->launches += 2 + 9 * (int64_t)b->sub.size();
+  CK(cudaStreamSynchronize(st));
+  for (ag_ctx* c : b->sub) {
+    c->checksumSplits = 0;
+    if (int e = checkStatus(c)) return e;
+  }
+  return AG_OK;
+}
+
+extern "C" int ag_batch_download(ag_batch* b, int i, float* out) {
+  if (!b || i < 0 || i >= (int)b->sub.size() || !out) return fail(AG_E_INVALID, "bad batch download");
+  ag_ctx* c = b->sub[i];
+  CK(cudaMemcpyAsync(out, c->maps.p, sizeof(float) * (size_t)(c->nMaps + 2) * c->npoints(), cudaMemcpyDeviceToHost,
+                     b->ctx->stream));
+  CK(cudaStreamSynchronize(b->ctx->stream));
+  return AG_OK;
+}
+
+extern "C" int ag_batch_autotune(ag_batch* b, const char* cache_path) {
+  if (!b) return fail(AG_E_INVALID, "null batch");
+  static const int kCand[][3] = {{2, 16, 8}, {4, 8, 8}, {1, 16, 16}, {2, 8, 16}, {4, 16, 4}};
+  const int ncand = sizeof(kCand) / sizeof(kCand[0]);
+  int choice[9];
+  for (int k = 0; k < 9; k++) choice[k] = -1;
+  if (cache_path && cache_path[0]) {
+    if (FILE* f = fopen(cache_path, "r")) {
+      int cls, x, y, z;
+      while (fscanf(f, "emap_tile class=%d tile=%d,%d,%d\n", &cls, &x, &y, &z) == 4)
+        for (int k = 0; k < ncand && cls >= 0 && cls < 9; k++)
+          if (kCand[k][0] == x && kCand[k][1] == y && kCand[k][2] == z) choice[cls] = k;
+      fclose(f);
+    }
+  }
+  cudaStream_t st = b->ctx->stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int cls = 0; cls < 9; cls++) {
+    if (choice[cls] >= 0) continue;
+    // The median-sized job of the class stands for it.
+    std::vector<std::pair<double, ag_ctx*>> js;
+    for (ag_ctx* c : b->sub)
+      if (batchSizeClass(c) == cls) js.push_back({(double)c->nAtoms * (double)c->npoints(), c});
+    if (js.empty()) continue;
+    std::sort(js.begin(), js.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+    ag_ctx* c = js[js.size() / 2].second;
+    float best = 1e30f;
+    for (int k = 0; k < ncand; k++) {
+      for (int d = 0; d < 3; d++) c->tile[d] = kCand[k][d];
+      if (int e = restageItems(c)) return e;
+      agk::EmapParams P;
+      if (int e = buildEmapParams(c, c->maps.p + (size_t)c->nMaps * c->npoints(), false, P)) return e;
+      float tms = 1e30f;
+      for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(e0, st);
+        if (agk::emap_launch(P, true, agk::kEmapKahan, P.nblocks, st) != cudaSuccess) return fail(AG_E_CUDA, "tuning launch failed");
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) tms = std::min(tms, ms);
+      }
+      if (tms < best) {
+        best = tms;
+        choice[cls] = k;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  for (ag_ctx* c : b->sub) {
+    const int k = choice[batchSizeClass(c)] >= 0 ? choice[batchSizeClass(c)] : 0;
+    for (int d = 0; d < 3; d++) c->tile[d] = kCand[k][d];
+    if (int e = restageItems(c)) return e;
+  }
+  if (cache_path && cache_path[0]) {
+    if (FILE* f = fopen(cache_path, "w")) {
+      for (int cls = 0; cls < 9; cls++)
+        if (choice[cls] >= 0)
+          fprintf(f, "emap_tile class=%d tile=%d,%d,%d\n", cls, kCand[choice[cls]][0], kCand[choice[cls]][1],
+                  kCand[choice[cls]][2]);
+      fclose(f);
+    }
+  }
+  return batchBuild(b);
+}
+
+extern "C" int ag_batch_free(ag_batch* b) {
+  if (!b) return AG_OK;
+  batchDropGraph(b);
+  b->ejobs.release();
+  b->eunits.release();
+  b->ajobs.release();
+  b->aunits.release();
+  b->counters.release();
+  for (ag_ctx* c : b->sub) ag_ctx_destroy(c);
+  delete b;
+  return AG_OK;
+}
 
 extern "C" int ag_problem_write(ag_problem* P) {
   if (!P || P->p.out.empty()) return fail(AG_E_INVALID, "no computed maps");

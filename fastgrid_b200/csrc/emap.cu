@@ -53,6 +53,8 @@ struct EmapSmem {
   float4 farA[kTile];             // w pre-multiplied by invEps[8191]
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
   int cnt[4][kThreads / 32];
+  double wpart[kThreads / 32];
+  int unit;                       // persistent batch kernel: the unit being processed
   uint64_t bar[2];
 };
 
@@ -143,12 +145,11 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
   }
 }
 
+// One work unit: CTA box `blk` of job P against atom split `split`.  Called
+// once per CTA by emap_kernel, and repeatedly by the persistent batch kernel.
 template <bool DDD, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
+__device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, const int split, EmapSmem& S) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int blk = blockIdx.x % P.nblocks, split = blockIdx.x / P.nblocks;
   const EmapBlock B = P.blocks[blk];
   const int a0 = split * P.chunk;
   const int a1 = min(P.n_atoms, a0 + P.chunk);
@@ -185,6 +186,7 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
   }
 
   float sum[kNX], cmp[kNX];
+  double wsum = 0.0;  // FP64 sum of the weights this thread converted (checksum)
 #pragma unroll
   for (int k = 0; k < kNX; k++) { sum[k] = 0.f; cmp[k] = 0.f; }
 
@@ -219,6 +221,7 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
     float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < nt) {
       double4 a = S.ring[slot][tid];
+      wsum += a.w;
       loc.x = (float)((a.x - B.ox) * 100.0);
       loc.y = (float)((a.y - B.oy) * 100.0);
       loc.z = (float)((a.z - B.oz) * 100.0);
@@ -363,6 +366,20 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
     __syncthreads();  // ring slot and atom lists are free again
   }
 
+  // Net-charge checksum: the first CTA of each atom split reports, in FP64,
+  // the sum of the weights of every atom that went through its tile ring.
+  if (blk == 0 && P.checksum) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
+    if (lane == 0) S.wpart[warp] = wsum;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int w = 0; w < kThreads / 32; w++) s += S.wpart[w];
+      P.checksum[split] = s;
+    }
+  }
+
   if (!active) return;
   const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;
 #pragma unroll
@@ -375,6 +392,45 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(EmapParams P) {
     else
       P.partial[(int64_t)split * P.npoints + row + x] = v;
   }
+}
+
+template <bool DDD, int MODE>
+__global__ void __launch_bounds__(kThreads, 2) emap_kernel(const __grid_constant__ EmapParams P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
+  emap_unit<DDD, MODE>(P, blockIdx.x % P.nblocks, blockIdx.x / P.nblocks, S);
+}
+
+// Persistent kernel over the work units of many jobs (a batch of receptors):
+// every CTA takes the next unit (job, CTA box) from an atomic counter until
+// none is left; the host orders units by decreasing cost.  Jobs run without
+// an atom split and with the distance-dependent dielectric.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2)
+    emap_batch_kernel(const EmapParams* __restrict__ jobs, const int2* __restrict__ units, int nunits, int* counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
+  for (;;) {
+    __syncthreads();  // the previous unit is finished by every thread
+    if (threadIdx.x == 0) S.unit = atomicAdd(counter, 1);
+    __syncthreads();
+    const int u = S.unit;
+    if (u >= nunits) return;
+    const int2 w = units[u];
+    emap_unit<true, MODE>(jobs[w.x], w.y, 0, S);
+  }
+}
+
+cudaError_t emap_batch_launch(const EmapParams* jobs, const int2* units, int nunits, int* counter, int grid,
+                              cudaStream_t st) {
+  const size_t smem = sizeof(EmapSmem);
+  cudaError_t e = cudaFuncSetAttribute(emap_batch_kernel<kEmapKahan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  emap_batch_kernel<kEmapKahan><<<grid, kThreads, smem, st>>>(jobs, units, nunits, counter);
+  return cudaGetLastError();
 }
 
 // Sum the atom-split partials in split order (FP64).

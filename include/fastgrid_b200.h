@@ -168,6 +168,28 @@ const float* ag_problem_maps(const ag_problem* p);
 /* Write every .map file (and the floating grid) like GridMapList::saveGridMap. */
 int ag_problem_write(ag_problem* p);
 
+/* ------------------------------------------------------------------------ */
+/* Batches: many map sets (receptors or conformations of uneven atom counts */
+/* and grid sizes) computed by persistent e-map and affinity kernels that   */
+/* take (job, CTA) work units from a counter, largest first; the first      */
+/* ag_batch_compute captures the whole batch in a CUDA graph and later calls*/
+/* replay it.  No counterpart in the reference (one job per process).       */
+/* Problems must outlive the batch; all use the distance-dependent          */
+/* dielectric.                                                               */
+/* ------------------------------------------------------------------------ */
+typedef struct ag_batch ag_batch;
+int ag_batch_create(ag_ctx* ctx, ag_problem* const* problems, int n, ag_batch** out);
+/* Choose the e-map CTA tile shape per size class (atom count x grid size) by
+ * timing candidates on one job of each class; cache_path (or NULL) names a
+ * text file of earlier choices that is read first and rewritten after. */
+int ag_batch_autotune(ag_batch* b, const char* cache_path);
+int ag_batch_compute(ag_batch* b);
+/* Map set of problem i: (n_maps + 2) * nx*ny*nz floats, as ag_download. */
+int ag_batch_download(ag_batch* b, int i, float* out);
+/* Sum over the batch of n_atoms x n_points (the batch's point-atom pairs). */
+double ag_batch_pairs(const ag_batch* b);
+int ag_batch_free(ag_batch* b);
+
 /* The autogrid4 / fastgrid4 command line (ProgramParameters.cpp:63-112). */
 int ag_main(int argc, char** argv);
 
