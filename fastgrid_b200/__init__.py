@@ -24,6 +24,9 @@ CLI_PATH = os.path.join(HERE, "_lib", "fastgrid4")
 
 AG_OK = 0
 AG_WORK_EMAP, AG_WORK_AFFINITY, AG_WORK_ALL = 1, 2, 3
+AG_WORK_EMAP_SURROGATE = 4
+SURROGATE_WEIGHTS = 35424
+DEFAULT_WEIGHTS = os.path.join(HERE, "surrogate_weights.bin")
 AG_EMAP_KAHAN, AG_EMAP_PLAIN = 0, 1
 AG_TUNE_EMAP_RNEAR, AG_TUNE_EMAP_ANALYTIC_EVERY, AG_TUNE_EMAP_CTAS_PER_SM = 1, 2, 3
 TABLE_LEN = 8192
@@ -67,13 +70,36 @@ class SynthParams(C.Structure):
                 ("dielectric", C.c_double)]
 
 
+class SurrogateParams(C.Structure):
+    _fields_ = [("r_near", C.c_double), ("coarse_spacing", C.c_double), ("probe_tol", C.c_double),
+                ("probes_per_box", C.c_int), ("use_corrector", C.c_int)]
+
+
+class SurrogateStats(C.Structure):
+    _fields_ = [("boxes", C.c_int), ("fallback_boxes", C.c_int), ("probe_max_err", C.c_double)]
+
+
+class SurrogateTrainParams(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_receptors", C.c_int), ("min_atoms", C.c_int), ("max_atoms", C.c_int),
+                ("points", C.c_int), ("spacing", C.c_double), ("epochs", C.c_int), ("lr", C.c_double)]
+
+
+class SurrogateTrainReport(C.Structure):
+    _fields_ = [("gen_seconds", C.c_double), ("train_seconds", C.c_double), ("steps", C.c_int),
+                ("first_epoch_loss", C.c_double), ("last_epoch_loss", C.c_double), ("s_in", C.c_double),
+                ("s_out", C.c_double)]
+
+
 # Every symbol include/fastgrid_b200.h declares.
 EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", "ag_ctx_launch_count",
            "ag_emap", "ag_emap_mode", "ag_affinity", "ag_upload", "ag_compute", "ag_device_maps", "ag_download",
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
            "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks",
            "ag_emap_noalloc", "ag_ctx_tune", "ag_batch_create", "ag_batch_autotune",
-           "ag_batch_compute", "ag_batch_download", "ag_batch_pairs", "ag_batch_free"]
+           "ag_batch_compute", "ag_batch_download", "ag_batch_pairs", "ag_batch_free", "ag_surrogate_set",
+           "ag_surrogate_load", "ag_surrogate_save", "ag_surrogate_weights", "ag_emap_surrogate",
+           "ag_surrogate_last_stats", "ag_surrogate_features", "ag_surrogate_net_grad", "ag_surrogate_train",
+           "ag_surrogate_receptor"]
 
 _lib = None
 
@@ -126,6 +152,16 @@ def lib():
     L.ag_batch_pairs.argtypes = [vp]
     L.ag_batch_pairs.restype = C.c_double
     L.ag_batch_free.argtypes = [vp]
+    L.ag_surrogate_set.argtypes = [vp, C.POINTER(SurrogateParams)]
+    L.ag_surrogate_load.argtypes = [vp, C.c_char_p]
+    L.ag_surrogate_save.argtypes = [vp, C.c_char_p]
+    L.ag_surrogate_weights.argtypes = [vp, fp, dp, fp, dp]
+    L.ag_emap_surrogate.argtypes = [vp, C.POINTER(Grid), C.c_int, dp, dp, fp, C.POINTER(SurrogateStats)]
+    L.ag_surrogate_last_stats.argtypes = [vp, C.POINTER(SurrogateStats)]
+    L.ag_surrogate_features.argtypes = [vp, C.POINTER(Grid), C.c_int, dp, dp, fp, fp]
+    L.ag_surrogate_net_grad.argtypes = [vp, C.POINTER(Grid), fp, fp, fp, fp, dp]
+    L.ag_surrogate_train.argtypes = [vp, C.POINTER(SurrogateTrainParams), C.POINTER(SurrogateTrainReport), dp]
+    L.ag_surrogate_receptor.argtypes = [C.c_uint64, C.c_int, dp]
     _lib = L
     return L
 
@@ -202,6 +238,88 @@ class Context:
 
     def device_maps(self):
         return lib().ag_device_maps(self.h)
+
+    # --- learned far-field surrogate of the e-map ---------------------------
+    def surrogate_set(self, r_near=10.0, coarse_spacing=1.5, probe_tol=0.005, probes_per_box=2, use_corrector=True):
+        p = SurrogateParams(r_near, coarse_spacing, probe_tol, probes_per_box, 1 if use_corrector else 0)
+        _check(lib().ag_surrogate_set(self.h, C.byref(p)))
+
+    def surrogate_load(self, path=DEFAULT_WEIGHTS):
+        _check(lib().ag_surrogate_load(self.h, path.encode()))
+
+    def surrogate_save(self, path):
+        _check(lib().ag_surrogate_save(self.h, path.encode()))
+
+    def surrogate_weights(self, w=None, scales=None):
+        """Set (if given) and return (FP32 weights, (s_in, s_out))."""
+        win = None if w is None else np.ascontiguousarray(w, dtype=np.float32)
+        sin = None if scales is None else np.ascontiguousarray(scales, dtype=np.float64)
+        wout = np.empty(SURROGATE_WEIGHTS, dtype=np.float32)
+        sout = np.empty(2, dtype=np.float64)
+        _check(lib().ag_surrogate_weights(self.h, None if win is None else _fp(win), None if sin is None else _dp(sin),
+                                          _fp(wout), _dp(sout)))
+        return wout, (float(sout[0]), float(sout[1]))
+
+    def emap_surrogate(self, grid, xyzw, inv_eps):
+        xyzw = np.ascontiguousarray(xyzw, dtype=np.float64)
+        eps = np.ascontiguousarray(inv_eps, dtype=np.float64)
+        out = np.empty(grid.nx * grid.ny * grid.nz, dtype=np.float32)
+        st = SurrogateStats()
+        _check(lib().ag_emap_surrogate(self.h, C.byref(grid), xyzw.shape[0], _dp(xyzw), _dp(eps), _fp(out),
+                                       C.byref(st)))
+        return out, dict(boxes=st.boxes, fallback_boxes=st.fallback_boxes, probe_max_err=st.probe_max_err)
+
+    def surrogate_stats(self):
+        st = SurrogateStats()
+        _check(lib().ag_surrogate_last_stats(self.h, C.byref(st)))
+        return dict(boxes=st.boxes, fallback_boxes=st.fallback_boxes, probe_max_err=st.probe_max_err)
+
+    def surrogate_features(self, grid, xyzw, inv_eps):
+        """(features (P, 8) FP32, base map (P,)) of the surrogate before its corrector."""
+        xyzw = np.ascontiguousarray(xyzw, dtype=np.float64)
+        eps = np.ascontiguousarray(inv_eps, dtype=np.float64)
+        n = grid.nx * grid.ny * grid.nz
+        feat = np.empty((n, 8), dtype=np.float32)
+        base = np.empty(n, dtype=np.float32)
+        _check(lib().ag_surrogate_features(self.h, C.byref(grid), xyzw.shape[0], _dp(xyzw), _dp(eps), _fp(feat),
+                                           _fp(base)))
+        return feat, base
+
+    def surrogate_net_grad(self, grid, features, target=None):
+        """(o, grad, loss) of the corrector on features (P, 8)."""
+        feat = np.ascontiguousarray(features, dtype=np.float32)
+        n = grid.nx * grid.ny * grid.nz
+        o = np.empty(n, dtype=np.float32)
+        grad = np.empty(SURROGATE_WEIGHTS, dtype=np.float32)
+        loss = C.c_double()
+        tgt = None if target is None else np.ascontiguousarray(target, dtype=np.float32)
+        _check(lib().ag_surrogate_net_grad(self.h, C.byref(grid), _fp(feat), None if tgt is None else _fp(tgt),
+                                           _fp(o), _fp(grad), C.byref(loss)))
+        return o, (grad if tgt is not None else None), loss.value
+
+    def surrogate_train(self, n_receptors=200, min_atoms=5000, max_atoms=30000, points=161, spacing=0.375,
+                        epochs=10, lr=2e-3, seed=1):
+        tp = SurrogateTrainParams(seed, n_receptors, min_atoms, max_atoms, points, spacing, epochs, lr)
+        rep = SurrogateTrainReport()
+        per = np.zeros(epochs, dtype=np.float64)
+        _check(lib().ag_surrogate_train(self.h, C.byref(tp), C.byref(rep), _dp(per)))
+        return dict(gen_seconds=rep.gen_seconds, train_seconds=rep.train_seconds, steps=rep.steps,
+                    first_epoch_loss=rep.first_epoch_loss, last_epoch_loss=rep.last_epoch_loss, s_in=rep.s_in,
+                    s_out=rep.s_out, loss_per_epoch=per.tolist())
+
+
+def surrogate_receptor(seed, n_atoms):
+    """(n, 4) atoms of the surrogate's synthetic receptor generator (centred, w = 0.1465 q)."""
+    out = np.empty((n_atoms, 4), dtype=np.float64)
+    _check(lib().ag_surrogate_receptor(seed, n_atoms, _dp(out)))
+    return out
+
+
+def ddd_table():
+    """332/eps(i/100) for i < 8192, the distance-dependent dielectric table (FP64)."""
+    d = np.arange(TABLE_LEN, dtype=np.float64) / 100.0
+    E = np.exp(-0.3153767175 * d)
+    return (332.0 + (332 * 7.7839) * E) / (78.4 + -66.57180475 * E)
 
 
 class Problem:

@@ -153,4 +153,16 @@ double roundOutput(double a);
 // Format `count` values (rounded like roundOutput) into `buf`; returns bytes.
 size_t formatValues(const float* v, int64_t count, char* buf);
 
+// 332/eps(r) of the Mehler-Solmajer dielectric (autogrid.h:233-239).
+double distDepDielInv(double d);
+}  // namespace ag
+
+struct ag_synth_params;
+namespace ag {
+// Seeded synthetic receptor (synth.cpp): 3-decimal coordinates, type codes
+// C OA N HD A SA = 0..5 and charges in thousandths.
+int synthReceptor(const ag_synth_params* sp, std::vector<double>& xyz, std::vector<int>& type,
+                  std::vector<long long>& milliCharge);
+const char* synthTypeName(int t);
+
 }  // namespace ag

@@ -41,9 +41,22 @@ struct EmapParams {
   double* partial;                // nsplit * npoints, when nsplit > 1
   unsigned* status;
   double* checksum;               // per split: FP64 sum of the weights the split's first CTA consumed (or null)
+  // Near-field mode of the far-field surrogate: only atoms within rcut of a
+  // point count, each as w * (exact term - psi(r)), psi(r) = (psi[0] +
+  // psi[1] r2 + psi[2] r2^2) / 100 with r2 in (0.01 A)^2 units.
+  float rcut2;                    // (100 * rcut)^2
+  float psi[3];
+  const float4* tileLo;           // near field: per 256-atom tile, bounding box of its atoms (A)
+  const float4* tileHi;
 };
 
 cudaError_t emap_launch(const EmapParams& P, bool ddd, int mode, int grid, cudaStream_t st);
+// Near field of the surrogate e-map (distance-dependent dielectric, Kahan).
+cudaError_t emap_near_launch(const EmapParams& P, int grid, cudaStream_t st);
+// Direct e-map of the CTA boxes list[0 .. *count) (no atom split), by `grid`
+// persistent CTAs; the surrogate's fallback for boxes whose probe failed.
+cudaError_t emap_list_launch(const EmapParams& P, const int* list, const int* count, int* counter, int grid,
+                             cudaStream_t st);
 size_t emap_smem_bytes();
 // Persistent e-map over the units (job, CTA box) of many jobs (no atom split, distance-dependent dielectric).
 cudaError_t emap_batch_launch(const EmapParams* jobs, const int2* units, int nunits, int* counter, int grid,

@@ -17,10 +17,11 @@
 #include <vector>
 
 #include "../../include/fastgrid_b200.h"
+#include "ag_ctx.h"
 #include "ag_host.h"
 #include "ag_kernels.h"
 
-namespace {
+namespace agc {
 
 thread_local std::string g_err;
 
@@ -33,32 +34,6 @@ int fail(int code, const char* fmt, ...) {
   g_err = buf;
   return code;
 }
-
-#define CK(call)                                                                          \
-  do {                                                                                    \
-    cudaError_t e_ = (call);                                                              \
-    if (e_ != cudaSuccess) return fail(AG_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-  } while (0)
-
-template <class T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t cap = 0;
-  cudaError_t ensure(size_t n) {
-    if (n <= cap && p) return cudaSuccess;
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
-    if (e == cudaSuccess) cap = std::max<size_t>(n, 1);
-    return e;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    cap = 0;
-  }
-};
 
 // Threshold table for the exact e-map bin: thr[k] is the least double r^2
 // with int(sqrt(r^2) * 100.0) >= k under IEEE double rounding, i.e. the bin
@@ -116,61 +91,13 @@ const std::vector<double>& affinityBinThresholds() {
   return thr;
 }
 
-}  // namespace
+}  // namespace agc
+
+using namespace agc;
 
 // ---------------------------------------------------------------------------
 // Context
 // ---------------------------------------------------------------------------
-struct ag_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int64_t launches = 0;
-  // e-map
-  DevBuf<double4> atoms;
-  DevBuf<float> epsTab;
-  DevBuf<double> thr;
-  DevBuf<int> items;
-  DevBuf<agk::EmapBlock> blocks;
-  DevBuf<double> partial;
-  DevBuf<float> maps;
-  DevBuf<unsigned> status;
-  std::vector<int> hItems;
-  std::vector<agk::EmapBlock> hBlocks;
-  int itemsFor[3] = {0, 0, 0};
-  double itemsH = 0;
-  int itemsTile = 0;
-  int tile[3] = {2, 16, 8};  // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
-  // affinity
-  DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
-  DevBuf<float> vol, solq, affTab, affTabH, sol, rv32, rv2_32;
-  DevBuf<double> rv64, thrA;
-  struct Pass {
-    int m0, nm, nmPad;
-    size_t tabOff, tabHOff;
-    unsigned typeModes[agk::kMaxTypes];
-    int typeNeedsAngular[agk::kMaxTypes];
-    int mapMinMaxSlot[agk::kMaxMapsPass];
-  };
-  std::vector<Pass> passes;
-  int typeHbond[agk::kMaxTypes] = {0};
-  // job
-  bool haveJob = false, haveAff = false, ddd = true;
-  ag_grid grid{};
-  int nAtoms = 0, nMaps = 0, nTypes = 0, hydrogen = -1;
-  double solparQ = 0;
-  std::vector<int> mapHbond, mapIsHB, mapCov;
-  std::vector<float> solparProbe, volProbe;
-  int emapMode = agk::kEmapKahan;
-  float rNear = 14.0f;
-  float delta = 2.0e-3f;
-  int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
-  int ctasPerSm = 2;
-  DevBuf<double> checksum;
-  int checksumSplits = 0;
-  double wSum = 0, wAbsSum = 0, lastChecksum = 0;
-  int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
-};
-
 extern "C" const char* ag_last_error(void) { return g_err.c_str(); }
 
 namespace ag {
@@ -217,6 +144,8 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   c->rv64.release();
   c->thrA.release();
   c->checksum.release();
+  agc::surrFree(c->surr);
+  c->surr = nullptr;
   c->blocks.release();
   c->status.release();
   for (auto* b : {&c->items, &c->info, &c->cellStart, &c->cellAtoms, &c->cellOf, &c->count, &c->fill, &c->dStart,
@@ -253,7 +182,7 @@ extern "C" int64_t ag_ctx_launch_count(const ag_ctx* c) { return c ? c->launches
 // ---------------------------------------------------------------------------
 // Job staging
 // ---------------------------------------------------------------------------
-namespace {
+namespace agc {
 
 int checkGrid(const ag_grid* g) {
   if (!g) return fail(AG_E_INVALID, "null grid");
@@ -264,19 +193,20 @@ int checkGrid(const ag_grid* g) {
 }
 
 // Work items of the e-map (NX points of one row each), grouped into CTAs of
-// 256 items walking 2 x 16 x 8 tiles of items, with each CTA's box.
-void buildItems(ag_ctx* c) {
-  const ag_grid& g = c->grid;
-  if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing &&
-      c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2])
-    return;
+// 256 items walking tiles of TX x TY x TZ items, with each CTA's box.
+// warpCompact: inside a tile, items go in blocks of TX x 4 x 4 (x fastest),
+// so each warp's 32 items form a compact box (for kernels that skip atoms
+// per warp); otherwise x, then y, then z.
+void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vector<int>& items,
+               std::vector<agk::EmapBlock>& blocks) {
   const int nxc = (g.nx + agk::kNX - 1) / agk::kNX;
-  const int TX = c->tile[0], TY = c->tile[1], TZ = c->tile[2];
-  c->hItems.clear();
+  const int TX = tile[0], TY = tile[1], TZ = tile[2];
+  items.clear();
   // Tiles in boustrophedon order (y rows and x columns reverse direction on
   // alternate passes), so a CTA that continues from one tile into the next
   // stays within neighbouring tiles and its box stays compact.
   const int ntx = (nxc + TX - 1) / TX, nty = (g.ny + TY - 1) / TY, ntz = (g.nz + TZ - 1) / TZ;
+  const bool compact = warpCompact && TY % 4 == 0 && TZ % 4 == 0;
   int serp = 0;
   for (int kz = 0; kz < ntz; kz++)
     for (int ky0 = 0; ky0 < nty; ky0++) {
@@ -284,21 +214,29 @@ void buildItems(ag_ctx* c) {
       for (int kx0 = 0; kx0 < ntx; kx0++, serp++) {
         const int kx = (serp / ntx) & 1 ? ntx - 1 - kx0 : kx0;
         const int tx = kx * TX, ty = ky * TY, tz = kz * TZ;
-        for (int z = tz; z < std::min(g.nz, tz + TZ); z++)
-          for (int y = ty; y < std::min(g.ny, ty + TY); y++)
-            for (int x = tx; x < std::min(nxc, tx + TX); x++) c->hItems.push_back(x | (y << 8) | (z << 19));
+        if (compact) {
+          for (int zb = tz; zb < tz + TZ; zb += 4)
+            for (int yb = ty; yb < ty + TY; yb += 4)
+              for (int z = zb; z < std::min(g.nz, zb + 4); z++)
+                for (int y = yb; y < std::min(g.ny, yb + 4); y++)
+                  for (int x = tx; x < std::min(nxc, tx + TX); x++) items.push_back(x | (y << 8) | (z << 19));
+        } else {
+          for (int z = tz; z < std::min(g.nz, tz + TZ); z++)
+            for (int y = ty; y < std::min(g.ny, ty + TY); y++)
+              for (int x = tx; x < std::min(nxc, tx + TX); x++) items.push_back(x | (y << 8) | (z << 19));
+        }
       }
     }
-  c->hBlocks.clear();
+  blocks.clear();
   const double h = g.spacing;
   const int n2x = g.nx / 2, n2y = g.ny / 2, n2z = g.nz / 2;
-  for (size_t i0 = 0; i0 < c->hItems.size(); i0 += 256) {
+  for (size_t i0 = 0; i0 < items.size(); i0 += 256) {
     agk::EmapBlock b{};
     b.item0 = (int)i0;
-    b.nitems = (int)std::min<size_t>(256, c->hItems.size() - i0);
+    b.nitems = (int)std::min<size_t>(256, items.size() - i0);
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int k = 0; k < b.nitems; k++) {
-      int v = c->hItems[i0 + k];
+      int v = items[i0 + k];
       int xc = v & 0xFF, y = (v >> 8) & 0x7FF, z = (v >> 19) & 0x7FF;
       int xa = xc * agk::kNX, xb = std::min(g.nx - 1, xa + agk::kNX - 1);
       double p[2][3] = {{(xa - n2x) * h, (y - n2y) * h, (z - n2z) * h}, {(xb - n2x) * h, (y - n2y) * h, (z - n2z) * h}};
@@ -320,8 +258,16 @@ void buildItems(ag_ctx* c) {
     const double rFar = std::max(50.0, std::min(60.0, 81.0 - diag));
     b.rfar2 = (float)((100.0 * rFar) * (100.0 * rFar));
     b.clampMid = rFar + diag >= 81.0 ? 1 : 0;  // mid-list bins may then exceed the table
-    c->hBlocks.push_back(b);
+    blocks.push_back(b);
   }
+}
+
+void buildItems(ag_ctx* c) {
+  const ag_grid& g = c->grid;
+  if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing &&
+      c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2])
+    return;
+  makeItems(g, c->tile, false, c->hItems, c->hBlocks);
   c->itemsFor[0] = g.nx;
   c->itemsFor[1] = g.ny;
   c->itemsFor[2] = g.nz;
@@ -347,8 +293,12 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
     }
     CK(c->atoms.ensure(n));
     if (n) CK(cudaMemcpyAsync(c->atoms.p, xyzw, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream));
+    c->atomsHost.assign(xyzw, xyzw + 4 * (size_t)n);
+    c->atomsVersion++;
   }
+  c->epsHost.clear();
   if (c->ddd) {
+    c->epsHost.assign(inv_eps, inv_eps + 8192);
     std::vector<float> t(8192);
     for (int i = 0; i < 8192; i++) t[i] = (float)inv_eps[i];
     CK(c->epsTab.ensure(8192));
@@ -689,7 +639,7 @@ int checkStatus(ag_ctx* c) {
   return AG_OK;
 }
 
-}  // namespace
+}  // namespace agc
 
 extern "C" int ag_upload(ag_ctx* c, const ag_grid* g, const ag_receptor* r, const ag_affinity_params* p,
                          const double* inv_eps) {
@@ -713,6 +663,8 @@ extern "C" int ag_compute(ag_ctx* c, int work) {
   float* maps = c->maps.p;
   if (work & AG_WORK_EMAP)
     if (int e = runEmap(c, maps + (size_t)c->nMaps * np)) return e;
+  if (work & AG_WORK_EMAP_SURROGATE)
+    if (int e = runEmapSurrogate(c, maps + (size_t)c->nMaps * np)) return e;
   if ((work & AG_WORK_AFFINITY) && c->haveAff)
     if (int e = runAffinity(c, maps, maps + (size_t)(c->nMaps + 1) * np)) return e;
   CK(cudaGetLastError());

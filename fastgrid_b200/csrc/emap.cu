@@ -433,6 +433,41 @@ cudaError_t emap_batch_launch(const EmapParams* jobs, const int2* units, int nun
   return cudaGetLastError();
 }
 
+// Persistent direct e-map over a device-side list of CTA boxes.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2)
+    emap_list_kernel(const __grid_constant__ EmapParams P, const int* __restrict__ list, const int* __restrict__ count,
+                     int* counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
+  const int n = min(*count, P.nblocks);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) S.unit = atomicAdd(counter, 1);
+    __syncthreads();
+    const int u = S.unit;
+    if (u >= n) return;
+    const int blk = list[u];
+    if (blk < 0 || blk >= P.nblocks) {
+      if (threadIdx.x == 0) atomicOr(P.status, ST_BAD_INPUT);
+      continue;
+    }
+    emap_unit<true, MODE>(P, blk, 0, S);
+  }
+}
+
+cudaError_t emap_list_launch(const EmapParams& P, const int* list, const int* count, int* counter, int grid,
+                             cudaStream_t st) {
+  const size_t smem = sizeof(EmapSmem);
+  cudaError_t e = cudaFuncSetAttribute(emap_list_kernel<kEmapKahan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+  emap_list_kernel<kEmapKahan><<<grid, kThreads, smem, st>>>(P, list, count, counter);
+  return cudaGetLastError();
+}
+
 // Sum the atom-split partials in split order (FP64).
 __global__ void emap_reduce_kernel(const double* __restrict__ partial, int nsplit, int64_t n, float* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {

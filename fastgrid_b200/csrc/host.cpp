@@ -13,6 +13,12 @@
 
 namespace ag {
 
+// 332/eps(r) for the Mehler-Solmajer dielectric (autogrid.h:233-239).
+double distDepDielInv(double d) {
+  double E = exp(-0.3153767175 * d);
+  return (332.0 + (332 * 7.7839) * E) / (78.4 + -66.57180475 * E);
+}
+
 // ---------------------------------------------------------------------------
 // Log
 // ---------------------------------------------------------------------------
@@ -270,11 +276,6 @@ int checkSize(int npts, char axis, Log& log) {
   return npts;
 }
 
-// 332/eps(r) for the Mehler-Solmajer dielectric (autogrid.h:233-239).
-double distDepDielInv(double d) {
-  double E = exp(-0.3153767175 * d);
-  return (332.0 + (332 * 7.7839) * E) / (78.4 + -66.57180475 * E);
-}
 
 void readReceptor(Problem& p, ParamLib& lib, Log& log, const char* fname, bool hasTypesLine,
                   int typesLineCount, double cmean[3]) {

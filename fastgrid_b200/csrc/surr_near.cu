@@ -1,0 +1,283 @@
+// Near field of the e-map surrogate: at every grid point, the exact binned
+// sum over the atoms within rcut (the direct kernel's near-path arithmetic:
+// 1/r capped at 2, the bin decided exactly in FP64 near a bin edge, Kahan
+// summation) minus the smooth kernel psi(r) for those atoms:
+//
+//   near(p) = sum_{r < rcut} w (min(1/r, 2) invEps[bin(r)] - psi(r)).
+//
+// The atoms arrive sorted along a Morton curve, so a 256-atom tile is a
+// compact blob; each CTA first lists the tiles whose bounding box lies within
+// rcut of its box and streams only those through shared memory (1-D TMA bulk
+// copies, two-slot ring, bounded mbarrier waits).  Inside a tile the atoms
+// within rcut of the CTA box form the near list; each warp then skips the
+// atoms farther than rcut from its own 32 work items' box.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "ag_device.cuh"
+#include "ag_kernels.h"
+
+namespace agk {
+
+using namespace agd;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTile = 256;
+constexpr int kTabLen = 8192;
+constexpr int kListCap = 1024;    // tiles listed per round (262,144 atoms)
+
+struct NearSmem {
+  float tab[kTabLen];
+  double4 ring[2][kTile];
+  float4 nearA[kTile];            // CTA-local x, y, z scaled by 100 and 100 w
+  short nearIdx[kTile];
+  int cnt[kThreads / 32];
+  int tileList[kListCap];
+  uint64_t bar[2];
+};
+
+// This thread's slot among the threads with `flag` set, in thread order;
+// `total` receives their count.  Contains two block-wide barriers.
+__device__ __forceinline__ int block_compact(bool flag, int* cnt, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) cnt[warp] = __popc(b);
+  __syncthreads();
+  int off = 0;
+  total = 0;
+#pragma unroll
+  for (int w = 0; w < kThreads / 32; w++) {
+    if (w == warp) off = total;
+    total += cnt[w];
+  }
+  __syncthreads();
+  return off + __popc(b & ((1u << lane) - 1u));
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_constant__ EmapParams P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  NearSmem& S = *reinterpret_cast<NearSmem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int blk = blockIdx.x % P.nblocks, split = blockIdx.x / P.nblocks;
+  const EmapBlock B = P.blocks[blk];
+  const int a0 = split * P.chunk;
+  const int a1 = min(P.n_atoms, a0 + P.chunk);
+  const int tl0 = a0 / kTile, tl1 = (a1 + kTile - 1) / kTile;  // the chunk is a multiple of kTile
+
+  // This thread's points, CTA-local and scaled by 100.
+  const bool active = tid < B.nitems;
+  const int v = P.items[B.item0 + (active ? tid : 0)];
+  const int xc = v & 0xFF, iy = (v >> 8) & 0x7FF, iz = (v >> 19) & 0x7FF;
+  const double h = P.h;
+  float gx[kNX];
+#pragma unroll
+  for (int k = 0; k < kNX; k++) gx[k] = (float)(((double)(xc * kNX + k - P.n2x) * h - B.ox) * 100.0);
+  const float gy = (float)(((double)(iy - P.n2y) * h - B.oy) * 100.0);
+  const float gz = (float)(((double)(iz - P.n2z) * h - B.oz) * 100.0);
+  // The box of this warp's points.
+  float wlo[3] = {gx[0], gy, gz}, whi[3] = {gx[kNX - 1], gy, gz};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      wlo[d] = fminf(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
+      whi[d] = fmaxf(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
+    }
+  const float warpCut2 = P.rcut2 * 1.0001f;
+
+  {
+    const float4* src = reinterpret_cast<const float4*>(P.table);
+    float4* dst = reinterpret_cast<float4*>(S.tab);
+    for (int i = tid; i < kTabLen / 4; i += kThreads) dst[i] = src[i];
+  }
+  if (tid == 0) {
+    mbar_init(&S.bar[0], 1);
+    mbar_init(&S.bar[1], 1);
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  float sum[kNX], cmp[kNX];
+#pragma unroll
+  for (int k = 0; k < kNX; k++) { sum[k] = 0.f; cmp[k] = 0.f; }
+  const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
+  const float kBias = 8388608.f;  // 2^23
+  const float rc = sqrtf(P.rcut2) * 0.01f + 0.01f;  // tile test radius (A), with a margin
+  const float bhx = B.hx * 0.01f, bhy = B.hy * 0.01f, bhz = B.hz * 0.01f;
+  unsigned seq = 0;  // tiles consumed: ring slot seq & 1, mbarrier phase (seq >> 1) & 1
+
+  for (int base = tl0; base < tl1; base += kListCap) {
+    const int bend = min(tl1, base + kListCap);
+    int ntl = 0;
+    for (int k0 = base; k0 < bend; k0 += kThreads) {
+      const int k = k0 + tid;
+      bool rel = false;
+      if (k < bend) {
+        const float4 lo = P.tileLo[k], hi = P.tileHi[k];
+        const float dx = fmaxf(fabsf(0.5f * (lo.x + hi.x) - (float)B.ox) - (0.5f * (hi.x - lo.x) + bhx), 0.f);
+        const float dy = fmaxf(fabsf(0.5f * (lo.y + hi.y) - (float)B.oy) - (0.5f * (hi.y - lo.y) + bhy), 0.f);
+        const float dz = fmaxf(fabsf(0.5f * (lo.z + hi.z) - (float)B.oz) - (0.5f * (hi.z - lo.z) + bhz), 0.f);
+        rel = dx * dx + dy * dy + dz * dz < rc * rc;
+      }
+      int tot;
+      const int pos = block_compact(rel, S.cnt, tot);
+      if (rel) S.tileList[ntl + pos] = k;
+      ntl += tot;
+    }
+    __syncthreads();
+    if (tid == 0 && ntl > 0) {
+      const int t0 = S.tileList[0] * kTile;
+      const unsigned n0 = (unsigned)min(kTile, a1 - t0);
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&S.bar[seq & 1], n0 * 32u);
+      tma_load_1d(S.ring[seq & 1], P.atoms + t0, n0 * 32u, &S.bar[seq & 1]);
+    }
+    for (int t = 0; t < ntl; t++, seq++) {
+      const int slot = seq & 1;
+      const int t0 = S.tileList[t] * kTile;
+      const int nt = min(kTile, a1 - t0);
+      if (tid == 0 && t + 1 < ntl) {
+        // The other slot was released by the barrier that ended the previous tile.
+        const int t1 = S.tileList[t + 1] * kTile;
+        const unsigned n1 = (unsigned)min(kTile, a1 - t1);
+        fence_proxy_async();
+        mbar_arrive_expect_tx(&S.bar[slot ^ 1], n1 * 32u);
+        tma_load_1d(S.ring[slot ^ 1], P.atoms + t1, n1 * 32u, &S.bar[slot ^ 1]);
+      }
+      const bool ok = mbar_wait_bounded(&S.bar[slot], (seq >> 1) & 1u, P.status);
+      if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+          mbar_wait_bounded(&S.bar[slot], (seq >> 1) & 1u, P.status);
+          if (t + 1 < ntl) mbar_wait_bounded(&S.bar[slot ^ 1], ((seq + 1) >> 1) & 1u, P.status);
+        }
+        return;
+      }
+      // Near list: atoms within rcut of the CTA box.
+      bool near = false;
+      float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (tid < nt) {
+        const double4 a = S.ring[slot][tid];
+        loc.x = (float)((a.x - B.ox) * 100.0);
+        loc.y = (float)((a.y - B.oy) * 100.0);
+        loc.z = (float)((a.z - B.oz) * 100.0);
+        loc.w = (float)(a.w * 100.0);
+        const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
+                    dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
+        near = dx * dx + dy * dy + dz * dz < P.rcut2;
+      }
+      int nNear;
+      const int pos = block_compact(near, S.cnt, nNear);
+      if (near) {
+        S.nearA[pos] = loc;
+        S.nearIdx[pos] = (short)tid;
+      }
+      __syncthreads();
+
+#pragma unroll 1
+      for (int j = 0; j < nNear; j++) {
+        const float4 a = S.nearA[j];
+        {  // skip atoms beyond rcut of every point of this warp (warp-uniform)
+          const float ex = fmaxf(fmaxf(wlo[0] - a.x, a.x - whi[0]), 0.f);
+          const float ey = fmaxf(fmaxf(wlo[1] - a.y, a.y - whi[1]), 0.f);
+          const float ez = fmaxf(fmaxf(wlo[2] - a.z, a.z - whi[2]), 0.f);
+          if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) >= warpCut2) continue;
+        }
+        const float dy = a.y - gy, dz = a.z - gz;
+        const float dyz2 = fmaf(dz, dz, dy * dy);
+        float rsv[kNX], fT[kNX], psi[kNX];
+        int idx[kNX];
+        unsigned flags = 0;
+#pragma unroll
+        for (int k = 0; k < kNX; k++) {
+          const float dx = a.x - gx[k];
+          const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
+          const float rs = rsqrt_approx(r2);
+          const bool in = r2 < P.rcut2;
+          rsv[k] = in ? rs : 0.f;
+          psi[k] = in ? fmaf(r2, fmaf(r2, P.psi[2], P.psi[1]), P.psi[0]) : 0.f;
+          const float T = r2 * rs;
+          fT[k] = T;
+          float f = __fmaf_rd(r2, rs, kBias);
+          f = fminf(f, kBias + (float)(kTabLen - 1));
+          idx[k] = __float_as_int(f) - 0x4B000000;
+          const float fr = T - (f - kBias);
+          if (in && fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
+        }
+        if (__any_sync(0xffffffffu, flags != 0)) {
+          if (flags) {
+            const double4 a64 = S.ring[slot][S.nearIdx[j]];
+            const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
+            const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
+            const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
+#pragma unroll
+            for (int k = 0; k < kNX; k++) {
+              if (flags & (1u << k)) {
+                const int kmid = min(__float_as_int(fT[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
+                const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
+                const double ddx = __dsub_rn(a64.x, gx64);
+                const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
+                idx[k] = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < kNX; k++) {
+          const float c = fminf(rsv[k], cap);
+          const float term = fmaf(-a.w, psi[k], (a.w * c) * S.tab[idx[k]]);
+          if (MODE == kEmapKahan) {
+            const float y = term - cmp[k];
+            const float s1 = sum[k] + y;
+            cmp[k] = (s1 - sum[k]) - y;
+            sum[k] = s1;
+          } else {
+            sum[k] += term;
+          }
+        }
+      }
+      __syncthreads();  // ring slot and near list are free again
+    }
+  }
+
+  if (!active) return;
+  const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;
+#pragma unroll
+  for (int k = 0; k < kNX; k++) {
+    const int x = xc * kNX + k;
+    if (x >= P.nx) break;
+    const double val = (MODE == kEmapKahan) ? (double)sum[k] - (double)cmp[k] : (double)sum[k];
+    if (P.nsplit == 1)
+      P.out[row + x] = (float)val;
+    else
+      P.partial[(int64_t)split * P.npoints + row + x] = val;
+  }
+}
+
+__global__ void surr_near_reduce_kernel(const double* __restrict__ partial, int nsplit, int64_t n,
+                                        float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int k = 0; k < nsplit; k++) s += partial[(int64_t)k * n + i];
+    out[i] = (float)s;
+  }
+}
+
+}  // namespace
+
+cudaError_t emap_near_launch(const EmapParams& P, int grid, cudaStream_t st) {
+  const size_t smem = sizeof(NearSmem);
+  cudaError_t e = cudaFuncSetAttribute(surr_near_kernel<kEmapKahan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  surr_near_kernel<kEmapKahan><<<grid, kThreads, smem, st>>>(P);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || P.nsplit == 1) return e;
+  surr_near_reduce_kernel<<<592, 256, 0, st>>>(P.partial, P.nsplit, P.npoints, P.out);
+  return cudaGetLastError();
+}
+
+}  // namespace agk

@@ -150,9 +150,12 @@ int repairTypes(const std::vector<double>& x, std::vector<int>& t) {
 }  // namespace
 }  // namespace ag
 
-extern "C" int ag_synth_write(const char* dir, const char* stem, const ag_synth_params* sp) {
-  using namespace ag;
-  if (!dir || !stem || !sp || sp->n_atoms <= 0) return AG_E_INVALID;
+namespace ag {
+
+// Atoms of a synthetic receptor: coordinates (3 decimals), type codes
+// (C OA N HD A SA = 0..5) and charges in thousandths.  Returns AG_OK or
+// AG_E_HOST when the shape is too full for the requested atom count.
+int synthReceptor(const ag_synth_params* sp, std::vector<double>& x, std::vector<int>& t, std::vector<long long>& k) {
   Rng rng(sp->seed);
   const int N = sp->n_atoms;
   Placer pl(sp->semi_axes, sp->origin, N);
@@ -190,13 +193,13 @@ extern "C" int ag_synth_write(const char* dir, const char* stem, const ag_synth_
   }
   // Quantise coordinates to what the PDBQT will hold before typing, so the
   // repair sees the same distances the loader will.
-  std::vector<double> x(pl.xyz);
+  x = pl.xyz;
   for (auto& v : x) v = std::round(v * 1000.0) / 1000.0;
 
   double fr[6] = {sp->frac_C, sp->frac_OA, sp->frac_N, sp->frac_HD, sp->frac_A, sp->frac_SA};
   double tot = 0;
   for (double f : fr) tot += f;
-  std::vector<int> t(N);
+  t.assign(N, 0);
   for (int i = 0; i < N; i++) {
     double u = rng.uni() * tot, c = 0;
     int k = 0;
@@ -217,7 +220,7 @@ extern "C" int ag_synth_write(const char* dir, const char* stem, const ag_synth_
     s += q[i];
   }
   double shift = (sp->net_charge - s) / N;
-  std::vector<long long> k(N);
+  k.assign(N, 0);
   long long ks = 0;
   for (int i = 0; i < N; i++) {
     k[i] = std::llround((q[i] + shift) * 1000.0);
@@ -233,6 +236,21 @@ extern "C" int ag_synth_write(const char* dir, const char* stem, const ag_synth_
     resid += resid > 0 ? -1 : 1;
   }
 
+  return AG_OK;
+}
+
+const char* synthTypeName(int t) { return kTypeName[t]; }
+
+}  // namespace ag
+
+extern "C" int ag_synth_write(const char* dir, const char* stem, const ag_synth_params* sp) {
+  using namespace ag;
+  if (!dir || !stem || !sp || sp->n_atoms <= 0) return AG_E_INVALID;
+  std::vector<double> x;
+  std::vector<int> t;
+  std::vector<long long> k;
+  if (int e = synthReceptor(sp, x, t, k)) return e;
+  const int N = sp->n_atoms;
   std::string base = std::string(dir) + "/" + stem;
   FILE* f = fopen((base + ".pdbqt").c_str(), "w");
   if (!f) return AG_E_HOST;

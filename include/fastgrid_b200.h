@@ -210,6 +210,83 @@ int ag_main(int argc, char** argv);
 int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps, float* d_out,
                     void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Learned far-field surrogate of the e-map (no reference counterpart; an   */
+/* approximate, faster alternative to ag_emap for the distance-dependent    */
+/* dielectric).  The map is split exactly into                              */
+/*   near field: the exact binned sum over atoms within r_near, minus a     */
+/*     smooth kernel psi for those atoms, and                               */
+/*   far field: the sum of psi over all atoms, sampled on a coarse grid,    */
+/*     interpolated trilinearly and corrected by a 3-layer 3x3x3            */
+/*     convolutional network (32 channels, BF16 weights, FP32 accumulation).*/
+/* Residual probes (the exact FP64 direct sum at a few points of every CTA  */
+/* box) send each box whose error exceeds probe_tol back to the direct sum. */
+/* ------------------------------------------------------------------------ */
+typedef struct ag_surrogate_params {
+  double r_near;               /* A, radius of the exact near field (default 10) */
+  double coarse_spacing;       /* A, far-field grid (default 1.5; rounded to a multiple of the map spacing) */
+  double probe_tol;            /* kcal/mol/e; <= 0 turns the probes and the fallback off (default 0.005) */
+  int probes_per_box;          /* probe points per CTA box (default 2) */
+  int use_corrector;           /* 0: trilinear far field only (default 1) */
+} ag_surrogate_params;
+typedef struct ag_surrogate_stats {
+  int boxes;                   /* CTA boxes of the last surrogate e-map */
+  int fallback_boxes;          /* boxes recomputed by the direct sum */
+  double probe_max_err;        /* largest probe error before the fallback (kcal/mol/e) */
+} ag_surrogate_stats;
+#define AG_SURROGATE_WEIGHTS 35424 /* W1 [27][8][32] | W2 [27][32][32] | W3 [27][32] */
+#define AG_WORK_EMAP_SURROGATE 4   /* ag_compute: the e-map slot by the surrogate */
+
+int ag_surrogate_set(ag_ctx* ctx, const ag_surrogate_params* p); /* NULL restores the defaults */
+/* Corrector weights file (BF16 weights and the input/output scales). */
+int ag_surrogate_load(ag_ctx* ctx, const char* path);
+int ag_surrogate_save(ag_ctx* ctx, const char* path);
+/* FP32 copies of the weights in (w_in) and out (w_out), either may be NULL;
+ * scales[0] = input scale, scales[1] = output scale, read (scales_in) and
+ * written (scales_out), either may be NULL. */
+int ag_surrogate_weights(ag_ctx* ctx, const float* w_in, const double* scales_in, float* w_out, double* scales_out);
+/* The e-map by the surrogate, host buffers, synchronous (like ag_emap). */
+int ag_emap_surrogate(ag_ctx* ctx, const ag_grid* grid, int n_atoms, const double* xyzw, const double* inv_eps,
+                      float* out, ag_surrogate_stats* stats);
+int ag_surrogate_last_stats(ag_ctx* ctx, ag_surrogate_stats* stats);
+/* Test hooks: the corrector's 8 input features per point (FP32 values of the
+ * BF16 inputs, scaled) and the map before the corrector (near + trilinear
+ * far field) of a job. */
+int ag_surrogate_features(ag_ctx* ctx, const ag_grid* grid, int n_atoms, const double* xyzw, const double* inv_eps,
+                          float* features, float* base);
+/* The network alone on features (P x 8, rounded to BF16 on upload): output
+ * o (P, in units of the output scale) and, with a target (P), the loss
+ * mean((o - target / s_out)^2) and its gradient with respect to the
+ * AG_SURROGATE_WEIGHTS weights.  Outputs may be NULL. */
+int ag_surrogate_net_grad(ag_ctx* ctx, const ag_grid* grid, const float* features, const float* target, float* o,
+                          float* grad, double* loss);
+
+/* Training on synthetic receptors (globules at 0.06 atoms/A^3, charges
+ * N(0, 0.2) clipped at 0.7, net 0), each e-map computed by the direct
+ * kernel; Adam on FP32 master weights, forward and backward on the GPU. */
+typedef struct ag_surrogate_train_params {
+  uint64_t seed;
+  int n_receptors;             /* e.g. 200 */
+  int min_atoms, max_atoms;    /* log-uniform atom counts, e.g. 5000 .. 30000 */
+  int points;                  /* grid points per axis, e.g. 161 */
+  double spacing;              /* A, e.g. 0.375 */
+  int epochs;
+  double lr;                   /* peak Adam learning rate, e.g. 2e-3 */
+} ag_surrogate_train_params;
+typedef struct ag_surrogate_train_report {
+  double gen_seconds;          /* receptors, direct e-maps and features */
+  double train_seconds;
+  int steps;
+  double first_epoch_loss, last_epoch_loss;
+  double s_in, s_out;
+} ag_surrogate_train_report;
+/* loss_per_epoch (or NULL) receives `epochs` mean training losses. */
+int ag_surrogate_train(ag_ctx* ctx, const ag_surrogate_train_params* tp, ag_surrogate_train_report* rep,
+                       double* loss_per_epoch);
+/* Write the atoms of the synthetic training/evaluation receptor generator:
+ * xyzw (n_atoms x 4: centred coordinates, q * 0.1465). */
+int ag_surrogate_receptor(uint64_t seed, int n_atoms, double* xyzw);
+
 /* Measured issue-rate peaks of a device (no reference counterpart; used for
  * the e-map's roofline): SFU reciprocal square roots per second and FP32 FMA
  * instructions per second, at the clocks the device runs at now. */
