@@ -1,16 +1,19 @@
 // Near field of the e-map surrogate: at every grid point, the exact binned
 // sum over the atoms within rcut (the direct kernel's near-path arithmetic:
-// 1/r capped at 2, the bin decided exactly in FP64 near a bin edge, Kahan
-// summation) minus the smooth kernel psi(r) for those atoms:
+// 1/r capped at 2, the bin decided exactly in FP64 near a bin edge) minus the
+// smooth kernel psi(r) for those atoms:
 //
 //   near(p) = sum_{r < rcut} w (min(1/r, 2) invEps[bin(r)] - psi(r)).
 //
 // The atoms arrive sorted along a Morton curve, so a 256-atom tile is a
 // compact blob; each CTA first lists the tiles whose bounding box lies within
 // rcut of its box and streams only those through shared memory (1-D TMA bulk
-// copies, two-slot ring, bounded mbarrier waits).  Inside a tile the atoms
-// within rcut of the CTA box form the near list; each warp then skips the
-// atoms farther than rcut from its own 32 work items' box.
+// copies, two-slot ring, bounded mbarrier waits).  The atoms of those tiles
+// within rcut of the CTA box are gathered into one near batch (FP32 local
+// coordinates plus the FP64 record for exact bin decisions), which the CTA
+// then sums behind a single barrier; each warp skips the atoms farther than
+// rcut from its own 32 work items' box.  Terms are summed in plain FP32 over
+// chunks of 16 atoms, the chunk sums Kahan-compensated.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -28,12 +31,14 @@ constexpr int kThreads = 256;
 constexpr int kTile = 256;
 constexpr int kTabLen = 8192;
 constexpr int kListCap = 1024;    // tiles listed per round (262,144 atoms)
+constexpr int kNearCap = 1024;    // near batch capacity (atoms)
+constexpr int kChunk = 16;        // atoms per plain-FP32 chunk sum
 
 struct NearSmem {
   float tab[kTabLen];
   double4 ring[2][kTile];
-  float4 nearA[kTile];            // CTA-local x, y, z scaled by 100 and 100 w
-  short nearIdx[kTile];
+  float4 nearA[kNearCap];         // CTA-local x, y, z scaled by 100 and 100 w
+  double4 nearD[kNearCap];        // the FP64 record, for exact bin decisions
   int cnt[kThreads / 32];
   int tileList[kListCap];
   uint64_t bar[2];
@@ -57,11 +62,93 @@ __device__ __forceinline__ int block_compact(bool flag, int* cnt, int& total) {
   return off + __popc(b & ((1u << lane) - 1u));
 }
 
-template <int MODE>
+// Sum the near batch into this thread's points: for each atom within rcut of
+// a point, w (min(1/r, 2) invEps[bin] - psi(r)); bins within P.delta of an
+// edge are decided exactly in FP64 from the atom's FP64 record.
+__device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& P, int n, const float (&gx)[kNX],
+                                           float gy, float gz, int xc, int iy, int iz, const float (&wlo)[3],
+                                           const float (&whi)[3], float (&sum)[kNX], float (&cmp)[kNX]) {
+  const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
+  const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
+  const float warpCut2 = P.rcut2 * 1.0001f;
+  const uint32_t tabBiased = smem_u32(S.tab) - 0x2C000000u;  // address(tab) - 4 * bits(2^23)
+  const double h = P.h;
+#pragma unroll 1
+  for (int j0 = 0; j0 < n; j0 += kChunk) {
+    float cs[kNX];
+#pragma unroll
+    for (int k = 0; k < kNX; k++) cs[k] = 0.f;
+    const int j1 = min(n, j0 + kChunk);
+#pragma unroll 1
+    for (int j = j0; j < j1; j++) {
+      const float4 a = S.nearA[j];
+      {  // skip atoms beyond rcut of every point of this warp (warp-uniform)
+        const float ex = fmaxf(fmaxf(wlo[0] - a.x, a.x - whi[0]), 0.f);
+        const float ey = fmaxf(fmaxf(wlo[1] - a.y, a.y - whi[1]), 0.f);
+        const float ez = fmaxf(fmaxf(wlo[2] - a.z, a.z - whi[2]), 0.f);
+        if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) >= warpCut2) continue;
+      }
+      const float dy = a.y - gy, dz = a.z - gz;
+      const float dyz2 = fmaf(dz, dz, dy * dy);
+      float rsv[kNX], r2v[kNX], psi[kNX];
+      uint32_t bits[kNX];
+      unsigned flags = 0;
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        const float dx = a.x - gx[k];
+        const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
+        const float rs = rsqrt_approx(r2);
+        rsv[k] = rs;
+        r2v[k] = r2;
+        psi[k] = fmaf(r2, fmaf(r2, P.psi[2], P.psi[1]), P.psi[0]);
+        float f = __fmaf_rd(r2, rs, kBias);
+        f = fminf(f, kBias + (float)(kTabLen - 1));
+        bits[k] = __float_as_uint(f);
+        const float fr = r2 * rs - (f - kBias);  // fraction of 100 r
+        if (r2 < P.rcut2 && fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
+      }
+      if (__any_sync(0xffffffffu, flags != 0)) {
+        if (flags) {
+          const double4 a64 = S.nearD[j];
+          const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
+          const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
+          const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
+#pragma unroll
+          for (int k = 0; k < kNX; k++) {
+            if (flags & (1u << k)) {
+              // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
+              const int kmid = min(__float_as_int(r2v[k] * rsv[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
+              const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
+              const double ddx = __dsub_rn(a64.x, gx64);
+              const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
+              const int b = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
+              bits[k] = 0x4B000000u + (uint32_t)b;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        float t;
+        asm("ld.shared.f32 %0, [%1];" : "=f"(t) : "r"(tabBiased + (bits[k] << 2)));
+        const float term = fmaf(-a.w, psi[k], (a.w * fminf(rsv[k], cap)) * t);
+        cs[k] += r2v[k] < P.rcut2 ? term : 0.f;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kNX; k++) {
+      const float y = cs[k] - cmp[k];
+      const float s1 = sum[k] + y;
+      cmp[k] = (s1 - sum[k]) - y;
+      sum[k] = s1;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_constant__ EmapParams P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   NearSmem& S = *reinterpret_cast<NearSmem*>(smem_raw);
-  const int tid = threadIdx.x, lane = tid & 31;
+  const int tid = threadIdx.x;
   const int blk = blockIdx.x % P.nblocks, split = blockIdx.x / P.nblocks;
   const EmapBlock B = P.blocks[blk];
   const int a0 = split * P.chunk;
@@ -87,7 +174,6 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
       wlo[d] = fminf(wlo[d], __shfl_xor_sync(0xffffffffu, wlo[d], o));
       whi[d] = fmaxf(whi[d], __shfl_xor_sync(0xffffffffu, whi[d], o));
     }
-  const float warpCut2 = P.rcut2 * 1.0001f;
 
   {
     const float4* src = reinterpret_cast<const float4*>(P.table);
@@ -104,11 +190,10 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
   float sum[kNX], cmp[kNX];
 #pragma unroll
   for (int k = 0; k < kNX; k++) { sum[k] = 0.f; cmp[k] = 0.f; }
-  const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
-  const float kBias = 8388608.f;  // 2^23
   const float rc = sqrtf(P.rcut2) * 0.01f + 0.01f;  // tile test radius (A), with a margin
   const float bhx = B.hx * 0.01f, bhy = B.hy * 0.01f, bhz = B.hz * 0.01f;
   unsigned seq = 0;  // tiles consumed: ring slot seq & 1, mbarrier phase (seq >> 1) & 1
+  int nBatch = 0;    // atoms in the near batch (block-uniform)
 
   for (int base = tl0; base < tl1; base += kListCap) {
     const int bend = min(tl1, base + kListCap);
@@ -141,7 +226,7 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
       const int t0 = S.tileList[t] * kTile;
       const int nt = min(kTile, a1 - t0);
       if (tid == 0 && t + 1 < ntl) {
-        // The other slot was released by the barrier that ended the previous tile.
+        // The other slot was last read before the barriers that ended the previous tile's compaction.
         const int t1 = S.tileList[t + 1] * kTile;
         const unsigned n1 = (unsigned)min(kTile, a1 - t1);
         fence_proxy_async();
@@ -156,92 +241,36 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
         }
         return;
       }
-      // Near list: atoms within rcut of the CTA box.
+      // Atoms within rcut of the CTA box join the near batch.
       bool near = false;
       float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
+      double4 a64 = make_double4(0.0, 0.0, 0.0, 0.0);
       if (tid < nt) {
-        const double4 a = S.ring[slot][tid];
-        loc.x = (float)((a.x - B.ox) * 100.0);
-        loc.y = (float)((a.y - B.oy) * 100.0);
-        loc.z = (float)((a.z - B.oz) * 100.0);
-        loc.w = (float)(a.w * 100.0);
+        a64 = S.ring[slot][tid];
+        loc.x = (float)((a64.x - B.ox) * 100.0);
+        loc.y = (float)((a64.y - B.oy) * 100.0);
+        loc.z = (float)((a64.z - B.oz) * 100.0);
+        loc.w = (float)(a64.w * 100.0);
         const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
                     dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
         near = dx * dx + dy * dy + dz * dz < P.rcut2;
       }
       int nNear;
-      const int pos = block_compact(near, S.cnt, nNear);
+      const int pos = block_compact(near, S.cnt, nNear);  // ends with a barrier: the ring slot is read
+      if (nBatch + nNear > kNearCap) {
+        near_batch(S, P, nBatch, gx, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
+        __syncthreads();
+        nBatch = 0;
+      }
       if (near) {
-        S.nearA[pos] = loc;
-        S.nearIdx[pos] = (short)tid;
+        S.nearA[nBatch + pos] = loc;
+        S.nearD[nBatch + pos] = a64;
       }
-      __syncthreads();
-
-#pragma unroll 1
-      for (int j = 0; j < nNear; j++) {
-        const float4 a = S.nearA[j];
-        {  // skip atoms beyond rcut of every point of this warp (warp-uniform)
-          const float ex = fmaxf(fmaxf(wlo[0] - a.x, a.x - whi[0]), 0.f);
-          const float ey = fmaxf(fmaxf(wlo[1] - a.y, a.y - whi[1]), 0.f);
-          const float ez = fmaxf(fmaxf(wlo[2] - a.z, a.z - whi[2]), 0.f);
-          if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) >= warpCut2) continue;
-        }
-        const float dy = a.y - gy, dz = a.z - gz;
-        const float dyz2 = fmaf(dz, dz, dy * dy);
-        float rsv[kNX], fT[kNX], psi[kNX];
-        int idx[kNX];
-        unsigned flags = 0;
-#pragma unroll
-        for (int k = 0; k < kNX; k++) {
-          const float dx = a.x - gx[k];
-          const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
-          const float rs = rsqrt_approx(r2);
-          const bool in = r2 < P.rcut2;
-          rsv[k] = in ? rs : 0.f;
-          psi[k] = in ? fmaf(r2, fmaf(r2, P.psi[2], P.psi[1]), P.psi[0]) : 0.f;
-          const float T = r2 * rs;
-          fT[k] = T;
-          float f = __fmaf_rd(r2, rs, kBias);
-          f = fminf(f, kBias + (float)(kTabLen - 1));
-          idx[k] = __float_as_int(f) - 0x4B000000;
-          const float fr = T - (f - kBias);
-          if (in && fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
-        }
-        if (__any_sync(0xffffffffu, flags != 0)) {
-          if (flags) {
-            const double4 a64 = S.ring[slot][S.nearIdx[j]];
-            const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
-            const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
-            const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
-#pragma unroll
-            for (int k = 0; k < kNX; k++) {
-              if (flags & (1u << k)) {
-                const int kmid = min(__float_as_int(fT[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
-                const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
-                const double ddx = __dsub_rn(a64.x, gx64);
-                const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
-                idx[k] = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
-              }
-            }
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < kNX; k++) {
-          const float c = fminf(rsv[k], cap);
-          const float term = fmaf(-a.w, psi[k], (a.w * c) * S.tab[idx[k]]);
-          if (MODE == kEmapKahan) {
-            const float y = term - cmp[k];
-            const float s1 = sum[k] + y;
-            cmp[k] = (s1 - sum[k]) - y;
-            sum[k] = s1;
-          } else {
-            sum[k] += term;
-          }
-        }
-      }
-      __syncthreads();  // ring slot and near list are free again
+      nBatch += nNear;
     }
   }
+  __syncthreads();
+  near_batch(S, P, nBatch, gx, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
 
   if (!active) return;
   const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;
@@ -249,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
   for (int k = 0; k < kNX; k++) {
     const int x = xc * kNX + k;
     if (x >= P.nx) break;
-    const double val = (MODE == kEmapKahan) ? (double)sum[k] - (double)cmp[k] : (double)sum[k];
+    const double val = (double)sum[k] - (double)cmp[k];
     if (P.nsplit == 1)
       P.out[row + x] = (float)val;
     else
@@ -270,10 +299,10 @@ __global__ void surr_near_reduce_kernel(const double* __restrict__ partial, int 
 
 cudaError_t emap_near_launch(const EmapParams& P, int grid, cudaStream_t st) {
   const size_t smem = sizeof(NearSmem);
-  cudaError_t e = cudaFuncSetAttribute(surr_near_kernel<kEmapKahan>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e =
+      cudaFuncSetAttribute(surr_near_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  surr_near_kernel<kEmapKahan><<<grid, kThreads, smem, st>>>(P);
+  surr_near_kernel<<<grid, kThreads, smem, st>>>(P);
   e = cudaGetLastError();
   if (e != cudaSuccess || P.nsplit == 1) return e;
   surr_near_reduce_kernel<<<592, 256, 0, st>>>(P.partial, P.nsplit, P.npoints, P.out);

@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(256) surr_coarse_kernel(const CoarseParams P) 
     gz = (float)((double)((K - G.halo) * G.R - G.n2z) * G.h);
   }
   const SplitKernel& S = P.K;
+  const float eShift = -S.negLambda2 * S.shift;
   const int split = blockIdx.y;
   const int a0 = split * P.chunk, a1 = min(P.n_atoms, a0 + P.chunk);
   double acc = 0.0;
@@ -65,8 +66,9 @@ __global__ void __launch_bounds__(256) surr_coarse_kernel(const CoarseParams P) 
         const float dx = a.x - gx, dy = a.y - gy, dz = a.z - gz;
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         const float rs = rsqrt_approx(fmaxf(r2, 1e-12f));
-        const float x = fminf(fmaf(r2, rs, -S.shift), S.xmax);
-        const float E = ex2f_approx(S.negLambda2 * x);
+        // E = exp(-lambda (r - shift)); past the table's end (81.91 A) the
+        // reference's value stays at bin 8191, which differs from this by < 1e-10.
+        const float E = ex2f_approx(fmaf(r2 * rs, S.negLambda2, eShift));
         const float tau =
             fmaf(E, fmaf(E, fmaf(E, fmaf(E, fmaf(E, S.poly[5], S.poly[4]), S.poly[3]), S.poly[2]), S.poly[1]),
                  S.poly[0]);
@@ -176,16 +178,20 @@ __global__ void surr_feature_kernel(const float4* __restrict__ rec, const SurrGe
 
 // ---------------------------------------------------------------------------
 // Tensor-core convolutions (mma.sync m16n8k16, BF16 x BF16 -> FP32).
-// Output tile 16 x 4 x 2 points per CTA iteration; each of the 8 warps owns
+// Output tile 16 x 4 x 4 points per CTA iteration; each of the 16 warps owns
 // one x row of 16 points (the MMA's M), the 3x3x3 taps and input channels
-// form K, the output channels N.  The input halo of a tile (18 x 6 x 4
-// points) and the packed weights sit in shared memory; fragments come from
-// ldmatrix, whose per-lane row addresses let a tap's shifted window be read
-// in place (no im2col copy).
+// form K, the output channels N.  The packed weights stay in shared memory
+// for the CTA's lifetime; input halos (18 x 6 x 6 points) are double-buffered
+// with cp.async, the next tile's halo landing while the current one is
+// multiplied.  Fragments come from ldmatrix, whose per-lane row addresses
+// read each tap's shifted window in place (no im2col copy); the K loop is
+// fully unrolled so every tap offset is an immediate.
 // ---------------------------------------------------------------------------
-constexpr int kTX = 16, kTY = 4, kTZ = 2;
+constexpr int kTX = 16, kTY = 4, kTZ = 4;
 constexpr int kHX = kTX + 2, kHY = kTY + 2, kHZ = kTZ + 2;
-constexpr int kHalo = kHX * kHY * kHZ;  // 432
+constexpr int kHalo = kHX * kHY * kHZ;     // 648
+constexpr int kTilePts = kTX * kTY * kTZ;  // 256
+constexpr int kConvThreads = 512;          // 16 warps, one x row each
 
 template <int CIN>
 struct ConvShape {
@@ -217,14 +223,27 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], 
       : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
+// 16-byte asynchronous copy global -> shared; src_bytes 0 fills zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ int tap_base(int t, int y, int z) {
   const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
   return ((z + dz) * kHY + (y + dy)) * kHX + dx;
 }
 
+__device__ __forceinline__ void tile_origin(int tile, int nx, int ny, int& x0, int& y0, int& z0) {
+  const int ntx = (nx + kTX - 1) / kTX, nty = (ny + kTY - 1) / kTY;
+  x0 = (tile % ntx) * kTX;
+  y0 = ((tile / ntx) % nty) * kTY;
+  z0 = (tile / (ntx * nty)) * kTZ;
+}
+
 // Halo of tile (x0, y0, z0) of a [P][CIN] BF16 tensor into sX (zero outside the grid).
-template <int CIN, int NTHREADS>
+template <int CIN, int NTHREADS, bool ASYNC>
 __device__ __forceinline__ void load_halo(const uint16_t* __restrict__ in, uint16_t* sX, int x0, int y0, int z0, int nx,
                                           int ny, int nz) {
   constexpr int CH = CIN / 8;
@@ -233,64 +252,90 @@ __device__ __forceinline__ void load_halo(const uint16_t* __restrict__ in, uint1
     const int pt = i / CH, c = i - pt * CH;
     const int hx = pt % kHX, hy = (pt / kHX) % kHY, hz = pt / (kHX * kHY);
     const int gx = x0 + hx - 1, gy = y0 + hy - 1, gz = z0 + hz - 1;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (gx >= 0 && gx < nx && gy >= 0 && gy < ny && gz >= 0 && gz < nz)
-      v = __ldg(reinterpret_cast<const uint4*>(in) + (((int64_t)gz * ny + gy) * nx + gx) * CH + c);
-    *reinterpret_cast<uint4*>(sX + pt * CS + c * 8) = v;
+    const bool inside = gx >= 0 && gx < nx && gy >= 0 && gy < ny && gz >= 0 && gz < nz;
+    const uint4* src = reinterpret_cast<const uint4*>(in) +
+                       (inside ? (((int64_t)gz * ny + gy) * nx + gx) * CH + c : 0);
+    if (ASYNC) {
+      cp_async16(smem_u32(sX + pt * CS + c * 8), src, inside ? 16 : 0);
+    } else {
+      *reinterpret_cast<uint4*>(sX + pt * CS + c * 8) = inside ? __ldg(src) : make_uint4(0u, 0u, 0u, 0u);
+    }
   }
 }
 
 template <int CIN, int NT, int EPI>
-__global__ void __launch_bounds__(256, 2) surr_conv_kernel(const ConvArgs A) {
+__global__ void __launch_bounds__(kConvThreads, 1) surr_conv_kernel(const ConvArgs A) {
   using SH = ConvShape<CIN>;
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* sW = reinterpret_cast<uint16_t*>(smem);  // [8 NT][KS]
-  uint16_t* sX = sW + 8 * NT * SH::KS;               // [kHalo][CS]
+  uint16_t* sX0 = sW + 8 * NT * SH::KS;              // two halo buffers [kHalo][CS]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int ntiles = ((A.nx + kTX - 1) / kTX) * ((A.ny + kTY - 1) / kTY) * ((A.nz + kTZ - 1) / kTZ);
+  if ((int)blockIdx.x < ntiles) {
+    int x0, y0, z0;
+    tile_origin(blockIdx.x, A.nx, A.ny, x0, y0, z0);
+    load_halo<CIN, kConvThreads, true>(A.in, sX0, x0, y0, z0, A.nx, A.ny, A.nz);
+  }
+  cp_async_commit();
   {
     const uint4* src = reinterpret_cast<const uint4*>(A.w);
     uint4* dst = reinterpret_cast<uint4*>(sW);
-    for (int i = tid; i < 8 * NT * SH::KS / 8; i += 256) dst[i] = __ldg(src + i);
+    for (int i = tid; i < 8 * NT * SH::KS / 8; i += kConvThreads) dst[i] = __ldg(src + i);
   }
-  const int ntx = (A.nx + kTX - 1) / kTX, nty = (A.ny + kTY - 1) / kTY, ntz = (A.nz + kTZ - 1) / kTZ;
-  const int ntiles = ntx * nty * ntz;
   const int q = lane >> 3, r = lane & 7, g = lane >> 2, tig = lane & 3;
   const int wy = warp & 3, wz = warp >> 2;
-  const uint32_t sWa = smem_u32(sW), sXa = smem_u32(sX);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * kTZ;
-    __syncthreads();  // the previous tile's fragments are read
-    load_halo<CIN, 256>(A.in, sX, x0, y0, z0, A.nx, A.ny, A.nz);
-    __syncthreads();
+  const uint32_t sWa = smem_u32(sW);
+  // Per-lane byte offsets of the A rows (tap 0) and B rows (chunk 0); the
+  // unrolled K loop adds compile-time tap and chunk offsets to them.
+  const uint32_t aLane =
+      (uint32_t)(((wz * kHY + wy) * kHX + r + ((q & 1) ? 8 : 0)) * SH::CS + (CIN == 32 && (q & 2) ? 8 : 0)) * 2u;
+  const bool aTap1 = CIN == 8 && (q & 2);  // CIN 8: lanes 16-31 read the second tap of a pair
+  const uint32_t bBase = NT == 1 ? sWa + (uint32_t)(r * SH::KS + (q & 1) * 8) * 2u
+                                 : sWa + (uint32_t)((8 * (q >> 1) + r) * SH::KS + (q & 1) * 8) * 2u;
+  int it = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, it++) {
+    uint16_t* sX = sX0 + (it & 1) * kHalo * SH::CS;
+    const int next = tile + gridDim.x;
+    if (next < ntiles) {
+      int nx0, ny0, nz0;
+      tile_origin(next, A.nx, A.ny, nx0, ny0, nz0);
+      load_halo<CIN, kConvThreads, true>(A.in, sX0 + ((it + 1) & 1) * kHalo * SH::CS, nx0, ny0, nz0, A.nx, A.ny,
+                                         A.nz);
+    }
+    cp_async_commit();
+    cp_async_wait1();  // this thread's copies of the current halo have landed
+    __syncthreads();   // ... and everyone else's (and the weights)
+    int x0, y0, z0;
+    tile_origin(tile, A.nx, A.ny, x0, y0, z0);
+    const uint32_t aBase = smem_u32(sX) + aLane;
     float acc[NT][4];
 #pragma unroll
     for (int n = 0; n < NT; n++) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
-#pragma unroll 2
+#pragma unroll
     for (int j = 0; j < SH::NCHUNK; j++) {
-      int pt, ch;
+      uint32_t aAddr;
       if (CIN == 32) {
         const int t = j >> 1;
-        pt = tap_base(t, wy, wz) + r + ((q & 1) ? 8 : 0);
-        ch = 16 * (j & 1) + ((q & 2) ? 8 : 0);
+        const int off = ((t / 9) * kHY + (t / 3) % 3) * kHX + t % 3;
+        aAddr = aBase + (uint32_t)(off * SH::CS + 16 * (j & 1)) * 2u;
       } else {
-        const int t = min(2 * j + ((q & 2) ? 1 : 0), 26);  // tap 27 is padding (zero weights)
-        pt = tap_base(t, wy, wz) + r + ((q & 1) ? 8 : 0);
-        ch = 0;
+        const int t0 = min(2 * j, 26), t1 = min(2 * j + 1, 26);  // tap 27 is padding (zero weights)
+        const int off0 = ((t0 / 9) * kHY + (t0 / 3) % 3) * kHX + t0 % 3;
+        const int off1 = ((t1 / 9) * kHY + (t1 / 3) % 3) * kHX + t1 % 3;
+        aAddr = aBase + (uint32_t)((aTap1 ? off1 : off0) * SH::CS) * 2u;
       }
       uint32_t a[4];
-      ldsm_x4(sXa + (uint32_t)(pt * SH::CS + ch) * 2u, a);
-      const int K0 = 16 * j;
+      ldsm_x4(aAddr, a);
+      const uint32_t K0b = 32u * j;  // 16 BF16 per chunk
       if (NT == 1) {
         uint32_t b0, b1;
-        ldsm_x2(sWa + (uint32_t)(r * SH::KS + K0 + (q & 1) * 8) * 2u, b0, b1);
+        ldsm_x2(bBase + K0b, b0, b1);
         mma_bf16(acc[0], a, b0, b1);
       } else {
 #pragma unroll
         for (int np = 0; np < NT / 2; np++) {
           uint32_t b[4];
-          const int co = 8 * (2 * np + (q >> 1)) + r;
-          ldsm_x4(sWa + (uint32_t)(co * SH::KS + K0 + (q & 1) * 8) * 2u, b);
+          ldsm_x4(bBase + K0b + (uint32_t)(16 * np * SH::KS) * 2u, b);
           mma_bf16(acc[2 * np], a, b[0], b[1]);
           mma_bf16(acc[2 * np + 1], a, b[2], b[3]);
         }
@@ -328,11 +373,12 @@ __global__ void __launch_bounds__(256, 2) surr_conv_kernel(const ConvArgs A) {
         }
       }
     }
+    __syncthreads();  // this halo buffer is read; the next iteration's prefetch may overwrite it
   }
 }
 
 // Weight gradient: per tap t, dW[t] (CIN x COUT) += X_t^T Y over the tile's
-// 128 points (K = points, fragments by transposing ldmatrix).  Units of work
+// 256 points (K = points, fragments by transposing ldmatrix).  Units of work
 // are (tap, 16 input channels) (CIN 32) or tap pairs (CIN 8), spread over 16
 // warps; accumulators stay in registers across all tiles a CTA visits and
 // are added to global memory once.
@@ -345,7 +391,7 @@ __global__ void __launch_bounds__(512, 1) surr_bwdw_kernel(const BwdwArgs A) {
   constexpr int COUT = NT == 1 ? 1 : 32;
   extern __shared__ __align__(16) unsigned char smem[];
   uint16_t* sX = reinterpret_cast<uint16_t*>(smem);  // [kHalo][CS]
-  uint16_t* sY = sX + kHalo * SH::CS;                // [128][YS]
+  uint16_t* sY = sX + kHalo * SH::CS;                // [kTilePts][YS]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int q = lane >> 3, r = lane & 7, g = lane >> 2, tig = lane & 3;
   const int ntx = (A.nx + kTX - 1) / kTX, nty = (A.ny + kTY - 1) / kTY, ntz = (A.nz + kTZ - 1) / kTZ;
@@ -357,13 +403,13 @@ __global__ void __launch_bounds__(512, 1) surr_bwdw_kernel(const BwdwArgs A) {
 #pragma unroll
     for (int n = 0; n < NT; n++) acc[u][n][0] = acc[u][n][1] = acc[u][n][2] = acc[u][n][3] = 0.f;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
-    const int x0 = tx * kTX, y0 = ty * kTY, z0 = tz * kTZ;
+    int x0, y0, z0;
+    tile_origin(tile, A.nx, A.ny, x0, y0, z0);
     __syncthreads();
-    load_halo<CIN, 512>(A.x, sX, x0, y0, z0, A.nx, A.ny, A.nz);
-    for (int i = tid; i < 128 * NT; i += 512) {
+    load_halo<CIN, 512, false>(A.x, sX, x0, y0, z0, A.nx, A.ny, A.nz);
+    for (int i = tid; i < kTilePts * NT; i += 512) {
       const int pt = i / NT, c = i - pt * NT;
-      const int lx = pt & 15, ly = (pt >> 4) & 3, lz = pt >> 6;
+      const int lx = pt % kTX, ly = (pt / kTX) % kTY, lz = pt / (kTX * kTY);
       const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (gx < A.nx && gy < A.ny && gz < A.nz)
@@ -376,8 +422,8 @@ __global__ void __launch_bounds__(512, 1) surr_bwdw_kernel(const BwdwArgs A) {
       const int u = warp + 16 * ui;
       if (u >= NU) continue;
 #pragma unroll 2
-      for (int kc = 0; kc < 8; kc++) {
-        const int ly = kc & 3, lz = kc >> 2;
+      for (int kc = 0; kc < kTY * kTZ; kc++) {
+        const int ly = kc % kTY, lz = kc / kTY;
         int pt, ch;
         if (CIN == 32) {
           pt = tap_base(u >> 1, ly, lz) + r + ((q & 2) ? 8 : 0);
@@ -559,34 +605,70 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
   return x;
 }
 
-// One warp per probe point: the exact FP64 direct sum, compared with the map.
-__global__ void surr_probe_kernel(const ProbeParams P) {
-  const int gw = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (gw >= P.nblocks * P.nprobe) return;
-  const int b = gw / P.nprobe, k = gw - b * P.nprobe;
-  const EmapBlock B = reinterpret_cast<const EmapBlock*>(P.blocks)[b];
-  if (B.nitems <= 0) return;
-  const uint32_t hsh = mix32((uint32_t)b * 7919u + (uint32_t)k * 104729u + 12345u);
-  const int seg = max(1, B.nitems / P.nprobe);
-  const int it = min(B.nitems - 1, k * seg + (int)(hsh % (uint32_t)seg));
-  const int v = P.items[B.item0 + it];
-  const int xc = v & 0xFF, y = (v >> 8) & 0x7FF, z = (v >> 19) & 0x7FF;
-  const int x = min(xc * kNX + (int)((hsh >> 16) % (uint32_t)kNX), P.nx - 1);
-  const double gx = (double)(x - P.n2x) * P.h, gy = (double)(y - P.n2y) * P.h, gz = (double)(z - P.n2z) * P.h;
-  double s = 0.0;
-  for (int i = lane; i < P.n_atoms; i += 32) {
-    const double4 a = P.atoms[i];
-    const double dx = a.x - gx, dy = a.y - gy, dz = a.z - gz;
-    const double r = sqrt(dx * dx + dy * dy + dz * dz);
-    const double inv = fmin(1.0 / r, 2.0);
-    const int bin = min((int)(r * 100.0), 8191);
-    s += a.w * inv * P.tab[bin];
+// One warp per probe point, eight per CTA sharing each 256-atom tile staged
+// in shared memory: the direct sum, compared with the map.  Pairs within 6 A
+// follow the reference's FP64 arithmetic (Cpu.cpp:59-82); farther pairs, where
+// a bin decided one step off moves a term by < 3e-5, run in FP32 with 1/r and
+// the bin from one reciprocal square root.
+__global__ void __launch_bounds__(256) surr_probe_kernel(const ProbeParams P) {
+  __shared__ double4 sA[256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gw = blockIdx.x * 8 + warp;
+  const bool valid = gw < P.nblocks * P.nprobe;
+  int b = 0, x = 0, y = 0, z = 0;
+  bool ok = false;
+  if (valid) {
+    b = gw / P.nprobe;
+    const int k = gw - b * P.nprobe;
+    const EmapBlock B = reinterpret_cast<const EmapBlock*>(P.blocks)[b];
+    if (B.nitems > 0) {
+      const uint32_t hsh = mix32((uint32_t)b * 7919u + (uint32_t)k * 104729u + 12345u);
+      const int seg = max(1, B.nitems / P.nprobe);
+      const int it = min(B.nitems - 1, k * seg + (int)(hsh % (uint32_t)seg));
+      const int v = P.items[B.item0 + it];
+      const int xc = v & 0xFF;
+      y = (v >> 8) & 0x7FF;
+      z = (v >> 19) & 0x7FF;
+      x = min(xc * kNX + (int)((hsh >> 16) % (uint32_t)kNX), P.nx - 1);
+      ok = true;
+    }
   }
+  const double gx = (double)(x - P.n2x) * P.h, gy = (double)(y - P.n2y) * P.h, gz = (double)(z - P.n2z) * P.h;
+  double s64 = 0.0;
+  float s = 0.f, c = 0.f;
+  for (int t0 = 0; t0 < P.n_atoms; t0 += 256) {
+    const int nt = min(256, P.n_atoms - t0);
+    __syncthreads();
+    if ((int)threadIdx.x < nt) sA[threadIdx.x] = P.atoms[t0 + threadIdx.x];
+    __syncthreads();
+    if (!ok) continue;
+    for (int i = lane; i < nt; i += 32) {
+      const double4 a = sA[i];
+      const double dx = a.x - gx, dy = a.y - gy, dz = a.z - gz;
+      const float fx = (float)dx, fy = (float)dy, fz = (float)dz;
+      const float r2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+      if (r2 < 36.f) {
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        const double inv = fmin(1.0 / r, 2.0);
+        const int bin = min((int)(r * 100.0), 8191);
+        s64 += a.w * inv * P.tab[bin];
+      } else {
+        const float rs = rsqrt_approx(r2);
+        const int bin = min((int)(r2 * rs * 100.f), 8191);
+        const float term = (float)a.w * rs * (float)P.tab[bin];
+        const float yk = term - c;  // Kahan
+        const float t = s + yk;
+        c = (t - s) - yk;
+        s = t;
+      }
+    }
+  }
+  s64 += (double)s - (double)c;
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) {
+  for (int o = 16; o > 0; o >>= 1) s64 += __shfl_xor_sync(0xffffffffu, s64, o);
+  if (ok && lane == 0) {
     const int64_t p = ((int64_t)z * P.ny + y) * P.nx + x;
-    const float err = (float)fabs((double)P.map[p] - s);
+    const float err = (float)fabs((double)P.map[p] - s64);
     atomicMax(P.maxErrBits, __float_as_uint(err));
     if (!(err <= P.tol)) {
       if (atomicExch(&P.flags[b], 1) == 0) P.list[atomicAdd(P.count, 1)] = b;
@@ -596,20 +678,25 @@ __global__ void surr_probe_kernel(const ProbeParams P) {
 
 template <int CIN, int NT, int EPI>
 cudaError_t conv_go(const ConvArgs& A, int sms, cudaStream_t st) {
-  const size_t smem = (size_t)(8 * NT * ConvShape<CIN>::KS + kHalo * ConvShape<CIN>::CS) * 2;
+  const size_t smem = (size_t)(8 * NT * ConvShape<CIN>::KS + 2 * kHalo * ConvShape<CIN>::CS) * 2;
   cudaError_t e = cudaFuncSetAttribute(surr_conv_kernel<CIN, NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;
   const int ntiles = ((A.nx + kTX - 1) / kTX) * ((A.ny + kTY - 1) / kTY) * ((A.nz + kTZ - 1) / kTZ);
-  const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
-  surr_conv_kernel<CIN, NT, EPI><<<grid, 256, smem, st>>>(A);
+  int per = 1;  // resident CTAs per SM
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, surr_conv_kernel<CIN, NT, EPI>, kConvThreads, smem) !=
+          cudaSuccess ||
+      per < 1)
+    per = 1;
+  const int grid = ntiles < per * sms ? ntiles : per * sms;
+  surr_conv_kernel<CIN, NT, EPI><<<grid, kConvThreads, smem, st>>>(A);
   return cudaGetLastError();
 }
 
 template <int CIN, int NT>
 cudaError_t bwdw_go(const BwdwArgs& A, int sms, cudaStream_t st) {
   constexpr int YS = NT == 1 ? 8 : 8 * NT + 8;
-  const size_t smem = (size_t)(kHalo * ConvShape<CIN>::CS + 128 * YS) * 2;
+  const size_t smem = (size_t)(kHalo * ConvShape<CIN>::CS + kTilePts * YS) * 2;
   cudaError_t e =
       cudaFuncSetAttribute(surr_bwdw_kernel<CIN, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -694,7 +781,7 @@ cudaError_t surr_scale_launch(uint4* feat, int64_t n, float s, cudaStream_t st) 
 cudaError_t surr_probe_launch(const ProbeParams& P, cudaStream_t st) {
   const int64_t warps = (int64_t)P.nblocks * P.nprobe;
   if (warps == 0) return cudaSuccess;
-  surr_probe_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(P);
+  surr_probe_kernel<<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(P);
   return cudaGetLastError();
 }
 

@@ -45,6 +45,7 @@ struct SurrState {
   DevBuf<double4> atomsSorted;
   DevBuf<float4> tileLo, tileHi;
   uint64_t sortedVersion = ~0ull;
+  std::vector<double> tab64Host;  // what S.tab64 holds
   int lastBoxes = 0;
   bool statsValid = false;
   void releaseAll() {
@@ -492,8 +493,11 @@ int runEmapSurrogate(ag_ctx* c, float* dOut) {
     CK(S.count.ensure(1));
     CK(S.counter.ensure(1));
     CK(S.maxErr.ensure(1));
-    CK(S.tab64.ensure(8192));
-    CK(cudaMemcpyAsync(S.tab64.p, c->epsHost.data(), sizeof(double) * 8192, cudaMemcpyHostToDevice, c->stream));
+    if (S.tab64Host != c->epsHost) {
+      CK(S.tab64.ensure(8192));
+      CK(cudaMemcpyAsync(S.tab64.p, c->epsHost.data(), sizeof(double) * 8192, cudaMemcpyHostToDevice, c->stream));
+      S.tab64Host = c->epsHost;
+    }
     CK(cudaMemsetAsync(S.flags.p, 0, sizeof(int) * nb, c->stream));
     CK(cudaMemsetAsync(S.count.p, 0, sizeof(int), c->stream));
     CK(cudaMemsetAsync(S.maxErr.p, 0, sizeof(unsigned), c->stream));
