@@ -12,6 +12,15 @@ write) between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+At N=1 the line also carries two supplementary measurements:
+  "surrogate": the learned far-field e-map surrogate against the direct e-map
+    on 20 held-out synthetic receptors (20,000 atoms, 161^3 grid, e-map only):
+    device time of both, speed-up, and the surrogate's error against the
+    direct sum over every point;
+  "batch": 64 receptors of 1,000-30,000 atoms on odd grids of 41^3-161^3
+    points with 6 ligand maps each, computed as one batch (persistent kernels
+    replayed from one CUDA graph, autotuned e-map tiles).
+
 --impl reference times FastGrid's own CPU path (oracle/_ref/fastgrid4, built
 from the reference sources, all host threads) on a bounded sample of the same
 workload (a 161 x 161 x 21 slab of the grid) and reports the same metric.
@@ -38,6 +47,117 @@ WORKLOAD = dict(n_atoms=20000, semi_axes=(45, 35, 30), npts=160, seed=2,
                 ligand_types="A C HD N NA OA SA S F Cl")
 SLAB_Z = 20          # CPU sample: npts 160 160 20 (161 x 161 x 21 points)
 REF_BIN = os.path.join(HERE, "oracle", "_ref", "fastgrid4")
+SURR_SEEDS = list(range(900001, 900021))   # held out: training uses seeds 1000003 * s + i
+# DRAM bytes of one emap_kernel launch on this workload (ncu dram__bytes_read.sum +
+# dram__bytes_write.sum): profiles/emap_kernel_20k_161.md.
+EMAP_TRAFFIC_BYTES = 3.10e6
+
+
+def surrogate_section(fg, torch, ctx, stream, flush, np):
+    """Direct vs surrogate e-map on the held-out receptors (device time, error)."""
+    import ctypes as C
+    g = fg.Grid(161, 161, 161, 0.375)
+    npts = g.nx * g.ny * g.nz
+    eps = fg.ddd_table()
+    eps_ptr = eps.ctypes.data_as(C.POINTER(C.c_double))
+    ctx.surrogate_load()
+    ctx.surrogate_set()
+    buf = np.empty(2 * npts, dtype=np.float32)
+    d_ms, s_ms, e2e_ms = [], [], []
+    max_err, sq, boxes, fallback, probe_max = 0.0, 0.0, 0, 0, 0.0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    for i, seed in enumerate(SURR_SEEDS):
+        x = fg.surrogate_receptor(seed, 20000)
+        rec = fg.Receptor()
+        rec.n_atoms = x.shape[0]
+        rec.xyzw = x.ctypes.data_as(C.POINTER(C.c_double))
+        ctx.upload(g, rec, None, eps_ptr)
+        for _ in range(3 if i == 0 else 1):  # warm-up
+            ctx.compute(fg.AG_WORK_EMAP)
+            ctx.compute(fg.AG_WORK_EMAP_SURROGATE)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+            ev[0].record(stream)
+            ctx.compute(fg.AG_WORK_EMAP)
+            ev[1].record(stream)
+        ctx.download(buf)
+        direct = buf[:npts].astype(np.float64)
+        with torch.cuda.stream(stream):
+            flush.fill_(2)
+            ev[2].record(stream)
+            ctx.compute(fg.AG_WORK_EMAP_SURROGATE)
+            ev[3].record(stream)
+        ctx.download(buf)
+        st = ctx.surrogate_stats()
+        d_ms.append(ev[0].elapsed_time(ev[1]))
+        s_ms.append(ev[2].elapsed_time(ev[3]))
+        err = np.abs(buf[:npts].astype(np.float64) - direct)
+        max_err = max(max_err, float(err.max()))
+        sq += float((err * err).sum())
+        boxes += st["boxes"]
+        fallback += st["fallback_boxes"]
+        probe_max = max(probe_max, st["probe_max_err"])
+        if i < 5:  # through the host-buffer entry point (atoms in, map out)
+            t0 = time.perf_counter()
+            ctx.emap_surrogate(g, x, eps)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    n = len(SURR_SEEDS)
+    dm, sm = sum(d_ms) / n, sum(s_ms) / n
+    pairs = 20000 * npts
+    return {"workload": f"{n} held-out synthetic receptors of 20000 atoms (globules at 0.06 atoms/A^3, charges "
+                        "N(0,0.2) clipped at 0.7, net 0), 161^3 grid @0.375 A, e-map only",
+            "direct_emap_ms": dm, "surrogate_emap_ms": sm, "speedup": dm / sm,
+            "direct_pairs_per_s": pairs / (dm * 1e-3), "surrogate_equiv_pairs_per_s": pairs / (sm * 1e-3),
+            "max_abs_err_vs_direct": max_err, "rms_err_vs_direct": (sq / (n * npts)) ** 0.5,
+            "stated_error_bound": 0.01, "boxes": boxes, "fallback_boxes": fallback,
+            "probe_max_err": probe_max, "e2e_ms_host_buffers": sum(e2e_ms) / len(e2e_ms),
+            "method": "exact near field within 10 A + 1.5 A far-field grid, trilinear + 3-layer 32-channel "
+                      "BF16 3D-conv corrector (shipped weights), residual probes with direct-sum fallback",
+            "l2": "flushed before each timed map"}
+
+
+def batch_section(fg, ctx, tmp, steps, np):
+    """64 receptors of uneven size as one batch under a captured CUDA graph."""
+    rng = np.random.default_rng(3)
+    d = os.path.join(tmp, "batch")
+    os.makedirs(d, exist_ok=True)
+    probs, atoms, grids = [], [], []
+    old = os.getcwd()
+    try:
+        for k in range(64):
+            n = int(round(np.exp(rng.uniform(np.log(1000), np.log(30000)))))
+            gsz = 2 * int(rng.integers(20, 81)) + 1
+            r = 20.0 * (n / 2000.0) ** (1 / 3)
+            fg.synth_write(d, f"j{k}", n_atoms=n, semi_axes=(r, r, r), npts=gsz - 1, seed=7000 + k,
+                           ligand_types="A C HD N OA SA")
+            os.chdir(d)
+            probs.append(fg.Problem(f"j{k}.gpf", log=f"j{k}.glg"))
+            os.chdir(old)
+            atoms.append(n)
+            grids.append(gsz)
+    finally:
+        os.chdir(old)
+    b = fg.Batch(ctx, probs)
+    t0 = time.perf_counter()
+    b.autotune(None)
+    tune_s = time.perf_counter() - t0
+    for _ in range(3):
+        b.compute()
+    ms = []
+    for _ in range(steps):
+        b.compute()
+        ms.append(b.last_ms)
+    pairs = b.pairs
+    b.close()
+    m = sum(ms) / len(ms)
+    return {"workload": "64 synthetic receptors, atoms log-uniform 1000-30000 (globules at 0.06 atoms/A^3), odd "
+                        "grids uniform 41^3-161^3 @0.375 A, ligand types A C HD N OA SA (6 maps + e + d)",
+            "atoms": [min(atoms), max(atoms)], "grid_points_per_axis": [min(grids), max(grids)],
+            "pairs": pairs, "ms_per_batch": m, "value": pairs / (m * 1e-3), "unit": UNIT,
+            "map_set_sec_mean": m * 1e-3 / 64, "autotune_s": tune_s,
+            "launch": "one CUDA graph: per-job cell lists, one persistent e-map kernel and one persistent affinity "
+                      "kernel over (job, CTA box) units, largest first"}
 
 
 def config_dict(n_gpus, extra=None):
@@ -162,6 +282,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -274,6 +396,13 @@ def main():
 
         emap_pairs_per_s = pairs / (emap_avg * 1e-3)
         ck = clocks.summary()
+
+        # ---- supplementary measurements (N=1) ----
+        surr = batch = None
+        if world == 1 and not args.no_surrogate:
+            surr = surrogate_section(fg, torch, ctx, stream, flush, np)
+        if world == 1 and not args.no_batch:
+            batch = batch_section(fg, ctx, tmp, args.steps, np)
         if rank == 0:
             line = {
                 "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -283,7 +412,8 @@ def main():
                 "map_set_sec": ms_step * 1e-3, "emap_ms": emap_avg, "affinity_ms": aff_avg,
                 "roofline": {"bound": "sfu", "kernel": "emap_kernel",
                              "achieved": emap_pairs_per_s / 1e9, "peak": rsqrt_ps / 1e9, "unit": "Gpair/s",
-                             "frac": emap_pairs_per_s / rsqrt_ps, "traffic": None,
+                             "frac": emap_pairs_per_s / rsqrt_ps, "traffic": EMAP_TRAFFIC_BYTES,
+                             "traffic_unit": "bytes per launch (ncu, profiles/emap_kernel_20k_161.md)",
                              "note": "one SFU rsqrt per point-atom pair; peak = rsqrt/s measured by "
                                      "ag_measure_peaks in this run (MEASURED_PEAKS.json has no SFU figure)"},
                 "roofline_fp32": {"achieved_ops": 8 * emap_pairs_per_s / 1e12, "peak": ffma_ps / 1e12,
@@ -292,7 +422,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_s * 1e3},
                 "gpu_launches": launches, "clocks": ck, "cpu_baseline": cpu,
-                "emap_abs_max": check,
+                "emap_abs_max": check, "surrogate": surr, "batch": batch,
             }
             print(json.dumps(line))
         ctx.close()

@@ -96,7 +96,7 @@ EXPORTS = ["ag_ctx_create", "ag_ctx_destroy", "ag_last_error", "ag_ctx_stream", 
            "ag_problem_load", "ag_problem_free", "ag_problem_info_get", "ag_problem_views", "ag_problem_compute",
            "ag_problem_maps", "ag_problem_write", "ag_main", "ag_synth_write", "ag_measure_peaks",
            "ag_emap_noalloc", "ag_ctx_tune", "ag_batch_create", "ag_batch_autotune",
-           "ag_batch_compute", "ag_batch_download", "ag_batch_pairs", "ag_batch_free", "ag_surrogate_set",
+           "ag_batch_compute", "ag_batch_download", "ag_batch_pairs", "ag_batch_last_ms", "ag_batch_free", "ag_surrogate_set",
            "ag_surrogate_load", "ag_surrogate_save", "ag_surrogate_weights", "ag_emap_surrogate",
            "ag_surrogate_last_stats", "ag_surrogate_features", "ag_surrogate_net_grad", "ag_surrogate_train",
            "ag_surrogate_receptor"]
@@ -151,6 +151,8 @@ def lib():
     L.ag_batch_download.argtypes = [vp, C.c_int, fp]
     L.ag_batch_pairs.argtypes = [vp]
     L.ag_batch_pairs.restype = C.c_double
+    L.ag_batch_last_ms.argtypes = [vp]
+    L.ag_batch_last_ms.restype = C.c_double
     L.ag_batch_free.argtypes = [vp]
     L.ag_surrogate_set.argtypes = [vp, C.POINTER(SurrogateParams)]
     L.ag_surrogate_load.argtypes = [vp, C.c_char_p]
@@ -403,6 +405,11 @@ class Batch:
     @property
     def pairs(self):
         return lib().ag_batch_pairs(self.h)
+
+    @property
+    def last_ms(self):
+        """Device time of the last compute()'s graph, in ms."""
+        return lib().ag_batch_last_ms(self.h)
 
     def maps(self, i):
         p = self.problems[i]

@@ -845,6 +845,8 @@ struct ag_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double pairs = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double lastMs = 0;                     // device time of the last graph launch
 };
 
 namespace {
@@ -985,15 +987,28 @@ extern "C" int ag_batch_compute(ag_batch* b) {
     b->graph = g;
     CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
   }
+  if (!b->ev[0]) {
+    CK(cudaEventCreate(&b->ev[0]));
+    CK(cudaEventCreate(&b->ev[1]));
+  }
+  CK(cudaEventRecord(b->ev[0], st));
   CK(cudaGraphLaunch(b->exec, st));
+  CK(cudaEventRecord(b->ev[1], st));
   b->ctx->launches += 2 + 9 * (int64_t)b->sub.size();
   CK(cudaStreamSynchronize(st));
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+    b->lastMs = ms;
+  }
   for (ag_ctx* c : b->sub) {
     c->checksumSplits = 0;
     if (int e = checkStatus(c)) return e;
   }
   return AG_OK;
 }
+
+extern "C" double ag_batch_last_ms(const ag_batch* b) { return b ? b->lastMs : 0.0; }
 
 extern "C" int ag_batch_download(ag_batch* b, int i, float* out) {
   if (!b || i < 0 || i >= (int)b->sub.size() || !out) return fail(AG_E_INVALID, "bad batch download");
@@ -1081,6 +1096,8 @@ extern "C" int ag_batch_free(ag_batch* b) {
   b->ajobs.release();
   b->aunits.release();
   b->counters.release();
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
   for (ag_ctx* c : b->sub) ag_ctx_destroy(c);
   delete b;
   return AG_OK;

@@ -188,6 +188,8 @@ int ag_batch_compute(ag_batch* b);
 int ag_batch_download(ag_batch* b, int i, float* out);
 /* Sum over the batch of n_atoms x n_points (the batch's point-atom pairs). */
 double ag_batch_pairs(const ag_batch* b);
+/* Device time in ms of the last ag_batch_compute's graph (CUDA events). */
+double ag_batch_last_ms(const ag_batch* b);
 int ag_batch_free(ag_batch* b);
 
 /* The autogrid4 / fastgrid4 command line (ProgramParameters.cpp:63-112). */
