@@ -221,6 +221,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def max_over_ranks(value, dist, device):
+    """Max of a per-rank float over all ranks (the value itself without a process group)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def fastgrid_cpu_run(workdir, gpf):
     """Run FastGrid's CPU build on `gpf`; return (map-set seconds, stderr)."""
     r = subprocess.run([REF_BIN, "-p", os.path.basename(gpf), "-l", "ref.glg", "--benchmark"], cwd=workdir,
@@ -349,11 +359,7 @@ def main():
         torch.cuda.synchronize()
         step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
         emap_ms = [s.elapsed_time(e) for s, e in zip(e_starts, e_ends)]
-        tot_ms = sum(step_ms)
-        if dist:
-            t = torch.tensor([tot_ms], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            tot_ms = float(t.item())
+        tot_ms = max_over_ranks(sum(step_ms), dist, f"cuda:{local}")
         ms_step = tot_ms / args.steps
         value = world * pairs / (ms_step * 1e-3)
         emap_avg = sum(emap_ms) / len(emap_ms)
@@ -378,11 +384,7 @@ def main():
             ctx.compute(fg.AG_WORK_ALL)
             ctx.download(outp)
             e2e_t.append(time.perf_counter() - t0)
-        e2e_s = sum(e2e_t) / len(e2e_t)
-        if dist:
-            t = torch.tensor([e2e_s], device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(sum(e2e_t) / len(e2e_t), dist, f"cuda:{local}")
         e2e_value = world * pairs / e2e_s
         check = float(np.abs(outp[nmaps * npts:(nmaps + 1) * npts]).max())
 

@@ -1,0 +1,128 @@
+"""CPU tests of the host side: the C ABI library loads and exports every
+function include/fastgrid_b200.h declares, the command line's exit codes
+follow the reference (ProgramParameters.cpp:103-107, ExitProgram(911)), the
+synthetic receptor generators keep their promises, and the benchmark's
+max-over-ranks timing works across two gloo ranks."""
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+import fastgrid_b200 as fg
+
+HEADER = os.path.join(REPO, "include", "fastgrid_b200.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(ag_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_function():
+    names = header_functions()
+    assert len(names) > 40
+    lib = fg.lib()
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(fg.EXPORTS) == names
+
+
+def test_cli_exit_codes(tmp_path):
+    exe = fg.CLI_PATH
+    r = subprocess.run([exe, "--no-such-switch"], capture_output=True, text=True)
+    assert r.returncode == 1 and "unknown switch" in r.stderr
+    r = subprocess.run([exe, "-p", str(tmp_path / "missing.gpf"), "-l", str(tmp_path / "x.glg")],
+                       capture_output=True, text=True)
+    assert r.returncode == 911 % 256  # ExitProgram(911), as the shell sees it
+    r = subprocess.run([exe, "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "--gpf" in r.stdout + r.stderr
+
+
+def _read_pdbqt(path):
+    xyz, q, t = [], [], []
+    for line in open(path):
+        if line.startswith("ATOM"):
+            xyz.append([float(line[30:38]), float(line[38:46]), float(line[46:54])])
+            q.append(float(line[70:76]))
+            t.append(line[77:].strip())
+    return np.array(xyz), np.array(q), t
+
+
+def _min_dist(x):
+    from scipy.spatial import cKDTree
+    d, _ = cKDTree(x).query(x, k=2)
+    return d[:, 1].min()
+
+
+def test_synth_write_properties(tmp_path):
+    fg.synth_write(str(tmp_path), "s", n_atoms=1500, semi_axes=(18, 16, 14), npts=40, seed=9, net_charge=2.0)
+    x, q, t = _read_pdbqt(tmp_path / "s.pdbqt")
+    assert len(x) == 1500
+    assert _min_dist(x) >= 1.2 - 2e-3
+    assert round(q.sum() * 1000) == 2000
+    assert set(t) <= {"C", "OA", "N", "HD", "A", "SA"}
+    # every HD sits next to an N/OA/SA within 20 atoms in file order (bond vectors need it)
+    for i, ti in enumerate(t):
+        if ti == "HD":
+            lo, hi = max(0, i - 20), min(len(t), i + 21)
+            d = np.linalg.norm(x[lo:hi] - x[i], axis=1)
+            assert np.any((d < 1.378) & (d > 0))
+    gpf = open(tmp_path / "s.gpf").read()
+    assert "npts 40 40 40" in gpf and "gridcenter auto" in gpf and "elecmap" in gpf
+
+
+def test_surrogate_receptor_generator():
+    x = fg.surrogate_receptor(123, 3000)
+    assert x.shape == (3000, 4)
+    assert abs(x[:, 3].sum()) < 1e-9                       # net charge 0
+    assert np.abs(x[:, :3].mean(axis=0)).max() < 1e-9      # centred on the centroid
+    assert _min_dist(x[:, :3]) >= 1.2 - 2e-3
+    r = 20.0 * (3000 / 2000.0) ** (1 / 3)
+    ext = x[:, :3].max(axis=0) - x[:, :3].min(axis=0)
+    assert np.all(ext <= 2 * r + 0.01)                     # inside a globule of radius r
+    np.testing.assert_array_equal(x, fg.surrogate_receptor(123, 3000))  # seeded
+
+
+def _rank(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    sys.path.insert(0, REPO)
+    import bench
+    out[rank] = bench.max_over_ranks(10.0 + 5.0 * rank, dist, "cpu")
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_max_over_ranks_two_gloo_ranks():
+    import socket
+    import torch.multiprocessing as mp
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert dict(out) == {0: 15.0, 1: 15.0}
+
+
+def test_bench_reference_arm_prints_only_on_rank0(capsys):
+    sys.path.insert(0, REPO)
+    import bench
+
+    class A:
+        steps, warmup, gpus = 1, 3, 2
+    assert bench.run_reference(A(), rank=1) is None
+    assert capsys.readouterr().out == ""
