@@ -67,7 +67,9 @@ struct ag_ctx {
   int itemsFor[3] = {0, 0, 0};
   double itemsH = 0;
   int itemsTile = 0;
-  int tile[3] = {2, 16, 8};  // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
+  int tile[3] = {1, 16, 16};  // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
+  bool warpCompact = true;    // e-map items in warp-compact order (see makeItems)
+  bool itemsCompact = false; // the order hItems was built with
   std::vector<double> epsHost;  // the staged 332/eps table (FP64), empty for the constant dielectric
   std::vector<double> atomsHost;  // host copy of the staged atoms (x, y, z, w)
   uint64_t atomsVersion = 0;      // bumped whenever new atoms are staged
@@ -92,7 +94,7 @@ struct ag_ctx {
   std::vector<int> mapHbond, mapIsHB, mapCov;
   std::vector<float> solparProbe, volProbe;
   int emapMode = agk::kEmapKahan;
-  float rNear = 14.0f;
+  float rNear = 11.0f;
   float delta = 2.0e-3f;
   int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
   int ctasPerSm = 2;

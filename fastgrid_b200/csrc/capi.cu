@@ -167,6 +167,19 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       if (!(v == 0.0 || (v >= 2.0 && v <= 64.0))) return fail(AG_E_INVALID, "analytic-every must be 0 or 2..64");
       c->anaEvery = (int)v;
       return AG_OK;
+    case AG_TUNE_EMAP_WARP_COMPACT:
+      if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "warp-compact item order must be 0 or 1");
+      c->warpCompact = v != 0.0;
+      return AG_OK;
+    case AG_TUNE_EMAP_TILE: {
+      const int t = (int)v, tx = t / 10000, ty = (t / 100) % 100, tz = t % 100;
+      if (v != (double)t || tx < 1 || ty < 1 || tz < 1 || tx * ty * tz != 256)
+        return fail(AG_E_INVALID, "tile must be TX*10000 + TY*100 + TZ with TX*TY*TZ = 256 work items");
+      c->tile[0] = tx;
+      c->tile[1] = ty;
+      c->tile[2] = tz;
+      return AG_OK;
+    }
     case AG_TUNE_EMAP_CTAS_PER_SM:
       if (!(v >= 1.0 && v <= 8.0)) return fail(AG_E_INVALID, "CTAs per SM must be 1..8");
       c->ctasPerSm = (int)v;
@@ -265,9 +278,10 @@ void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vecto
 void buildItems(ag_ctx* c) {
   const ag_grid& g = c->grid;
   if (c->itemsFor[0] == g.nx && c->itemsFor[1] == g.ny && c->itemsFor[2] == g.nz && c->itemsH == g.spacing &&
-      c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2])
+      c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2] && c->itemsCompact == c->warpCompact)
     return;
-  makeItems(g, c->tile, false, c->hItems, c->hBlocks);
+  makeItems(g, c->tile, c->warpCompact, c->hItems, c->hBlocks);
+  c->itemsCompact = c->warpCompact;
   c->itemsFor[0] = g.nx;
   c->itemsFor[1] = g.ny;
   c->itemsFor[2] = g.nz;

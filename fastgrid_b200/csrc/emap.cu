@@ -98,8 +98,9 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // ANALYTIC = true: the same value is evaluated on the FMA and SFU pipes,
 //   invEps(bin) = 332 (1 + a E) / (78.4 - c E),  E = exp(-0.3153767175 bin / 100)
 //   (autogrid.h:233-239), as the series sum_n P.poly[n] E^n; mid atoms are
-//   at least 14 A away, so E <= 0.0121 and the truncation is below 1e-8
-//   relative.  Running part of the atoms this way takes load off the
+//   at least rNear (default 11 A) away, so E <= 0.031 and the truncation is
+//   below 1e-8 relative (1e-6 at the smallest allowed rNear, 8 A).  Running
+//   part of the atoms this way takes load off the
 //   shared-memory pipe, whose random-bank table reads limit the kernel.
 // CLAMP: the CTA's box is large enough that a bin can pass the table's end.
 template <int MODE, bool CLAMP, bool ANALYTIC>
