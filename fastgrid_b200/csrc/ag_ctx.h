@@ -120,5 +120,7 @@ int runEmap(ag_ctx* c, float* dOut);
 int checkStatus(ag_ctx* c);
 // The e-map of the staged job by the learned far-field surrogate (surrogate_host.cu).
 int runEmapSurrogate(ag_ctx* c, float* dOut);
+// Run the surrogate's inference convolutions on tcgen05 (true) or mma.sync.
+void surrUseTc(ag_ctx* c, bool on);
 
 }  // namespace agc

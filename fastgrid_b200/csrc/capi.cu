@@ -180,6 +180,10 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       c->tile[2] = tz;
       return AG_OK;
     }
+    case AG_TUNE_SURROGATE_TCGEN05:
+      if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "tcgen05 switch must be 0 or 1");
+      agc::surrUseTc(c, v != 0.0);
+      return AG_OK;
     case AG_TUNE_EMAP_CTAS_PER_SM:
       if (!(v >= 1.0 && v <= 8.0)) return fail(AG_E_INVALID, "CTAs per SM must be 1..8");
       c->ctasPerSm = (int)v;

@@ -103,6 +103,17 @@ struct PackedWeights {
 };
 cudaError_t surr_pack_launch(const float* w, const PackedWeights& pw, cudaStream_t st);
 
+// tcgen05 forward convolutions (surr_tc.cu).  Weights in the tcgen05 layout:
+// layer 1 (8 -> 32, K padded to 16 per tap), 2 (32 -> 32), 3 (32 -> 1, N padded
+// to 16); surr_tc_weight_elems gives their BF16 element counts.
+size_t surr_tc_weight_elems(int layer);
+cudaError_t surr_pack_tc_launch(const float* w, uint16_t* w1, uint16_t* w2, uint16_t* w3, cudaStream_t st);
+// layer 1 and 2: EPI_LEAKY into out16; layer 3: EPI_ADD / EPI_STORE into outF.
+// Activations (in and out16) are chunk-planar [C/8][nz][ny][nx][8] (for the 8
+// feature channels the same as [P][8]).
+cudaError_t surr_conv_tc_launch(int layer, int epi, const ConvArgs& A, const uint16_t* wtc, unsigned* status, int sms,
+                                cudaStream_t st);
+
 // Training: loss = mean (o - y / sOut)^2; dO8[p] = (2 (o - y/sOut) / n, 0 x 7) in BF16.
 cudaError_t surr_loss_launch(const float* o, const float* y, int64_t n, float invSOut, uint4* do8, double* loss,
                              cudaStream_t st);

@@ -29,6 +29,8 @@ struct SurrState {
   bool packedValid = false;
   DevBuf<float> dW, dGrad, dM, dV, o, tgt;
   DevBuf<uint16_t> wk1, wk2, wk3, wk2t, wk3t;
+  DevBuf<uint16_t> wtc1, wtc2, wtc3;  // tcgen05 layouts
+  bool useTc = true;                  // inference convolutions on tcgen05 (mma.sync when false)
   DevBuf<double> cPartial, field, tab64, loss, sums;
   DevBuf<float4> rec;
   DevBuf<uint4> feat, do8;
@@ -50,7 +52,7 @@ struct SurrState {
   bool statsValid = false;
   void releaseAll() {
     for (auto* b : {&dW, &dGrad, &dM, &dV, &o, &tgt}) b->release();
-    for (auto* b : {&wk1, &wk2, &wk3, &wk2t, &wk3t, &a1, &a2, &dz1, &dz2}) b->release();
+    for (auto* b : {&wk1, &wk2, &wk3, &wk2t, &wk3t, &a1, &a2, &dz1, &dz2, &wtc1, &wtc2, &wtc3}) b->release();
     for (auto* b : {&cPartial, &field, &tab64, &loss, &sums}) b->release();
     rec.release();
     feat.release();
@@ -63,6 +65,8 @@ struct SurrState {
     tileHi.release();
   }
 };
+
+void surrUseTc(ag_ctx* c, bool on);
 
 void surrFree(SurrState* s) {
   if (!s) return;
@@ -195,7 +199,11 @@ int packWeights(ag_ctx* c, SurrState& S) {
   CK(cudaMemcpyAsync(S.dW.p, S.w.data(), sizeof(float) * agk::kSurrWeights, cudaMemcpyHostToDevice, c->stream));
   agk::PackedWeights pw{S.wk1.p, S.wk2.p, S.wk3.p, S.wk2t.p, S.wk3t.p};
   CK(agk::surr_pack_launch(S.dW.p, pw, c->stream));
-  c->launches += 1;
+  CK(S.wtc1.ensure(agk::surr_tc_weight_elems(1)));
+  CK(S.wtc2.ensure(agk::surr_tc_weight_elems(2)));
+  CK(S.wtc3.ensure(agk::surr_tc_weight_elems(3)));
+  CK(agk::surr_pack_tc_launch(S.dW.p, S.wtc1.p, S.wtc2.p, S.wtc3.p, c->stream));
+  c->launches += 2;
   CK(cudaStreamSynchronize(c->stream));
   S.packedValid = true;
   return AG_OK;
@@ -344,13 +352,31 @@ int surrBase(ag_ctx* c, SurrState& S, float* dBase, uint4* dFeat, float sIn) {
 }
 
 // Corrector forward: outF = scale * net(feat) (add: += instead of =).
-int surrNet(ag_ctx* c, SurrState& S, const agk::SurrGeom& G, const uint4* feat, float* outF, bool add, float scale) {
+// training: keep the activations in the [P][32] layout the backward kernels
+// read (mma.sync forward); otherwise tcgen05 when enabled (chunk-planar).
+int surrNet(ag_ctx* c, SurrState& S, const agk::SurrGeom& G, const uint4* feat, float* outF, bool add, float scale,
+            bool training) {
   if (int e = packWeights(c, S)) return e;
   const int n = sms(c);
   agk::ConvArgs A{};
   A.nx = G.nx;
   A.ny = G.ny;
   A.nz = G.nz;
+  if (S.useTc && !training) {  // tcgen05: accumulators in tensor memory
+    A.in = reinterpret_cast<const uint16_t*>(feat);
+    A.out16 = S.a1.p;
+    CK(agk::surr_conv_tc_launch(1, agk::EPI_LEAKY, A, S.wtc1.p, c->status.p, n, c->stream));
+    A.in = S.a1.p;
+    A.out16 = S.a2.p;
+    CK(agk::surr_conv_tc_launch(2, agk::EPI_LEAKY, A, S.wtc2.p, c->status.p, n, c->stream));
+    A.in = S.a2.p;
+    A.out16 = nullptr;
+    A.outF = outF;
+    A.scale = scale;
+    CK(agk::surr_conv_tc_launch(3, add ? agk::EPI_ADD : agk::EPI_STORE, A, S.wtc3.p, c->status.p, n, c->stream));
+    c->launches += 3;
+    return AG_OK;
+  }
   A.in = reinterpret_cast<const uint16_t*>(feat);
   A.w = S.wk1.p;
   A.out16 = S.a1.p;
@@ -482,7 +508,7 @@ int runEmapSurrogate(ag_ctx* c, float* dOut) {
   if (int e = surrBase(c, S, dOut, S.feat.p, S.sIn)) return e;
   if (S.par.use_corrector) {
     if (int e = ensureNet(S, np)) return e;
-    if (int e = surrNet(c, S, G, S.feat.p, dOut, true, S.sOut)) return e;
+    if (int e = surrNet(c, S, G, S.feat.p, dOut, true, S.sOut, false)) return e;
   }
   S.lastBoxes = (int)S.hBlocks.size();
   S.statsValid = false;
@@ -535,6 +561,8 @@ int runEmapSurrogate(ag_ctx* c, float* dOut) {
   }
   return AG_OK;
 }
+
+void surrUseTc(ag_ctx* c, bool on) { surrOf(c).useTc = on; }
 
 }  // namespace agc
 
@@ -727,7 +755,7 @@ extern "C" int ag_surrogate_net_grad(ag_ctx* c, const ag_grid* g, const float* f
   G.nx = g->nx;
   G.ny = g->ny;
   G.nz = g->nz;
-  if (int e = surrNet(c, S, G, S.feat.p, S.o.p, false, 1.f)) return e;
+  if (int e = surrNet(c, S, G, S.feat.p, S.o.p, false, 1.f, true)) return e;
   if (target) {
     CK(cudaMemcpyAsync(S.tgt.p, target, sizeof(float) * np, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(S.loss.p, 0, sizeof(double), c->stream));
@@ -864,7 +892,7 @@ extern "C" int ag_surrogate_train(ag_ctx* c, const ag_surrogate_train_params* tp
     for (int k = 0; k < nr; k++, step++) {
       const int i = order[k];
       const uint4* f = featAll.p + (size_t)i * np;
-      if (int e = surrNet(c, S, G, f, S.o.p, false, 1.f)) { cleanup(); return e; }
+      if (int e = surrNet(c, S, G, f, S.o.p, false, 1.f, true)) { cleanup(); return e; }
       CK(agk::surr_loss_launch(S.o.p, yAll.p + (size_t)i * np, np, 1.f / S.sOut, S.do8.p, lossSteps.p + step,
                                c->stream));
       if (int e = surrBackward(c, S, G, f)) { cleanup(); return e; }

@@ -121,3 +121,23 @@ def test_probe_fallback_reproduces_direct_sum():
     ctx.close()
     assert st["fallback_boxes"] == st["boxes"] > 0
     assert np.max(np.abs(out.astype(np.float64) - direct)) <= 1e-4
+
+
+def test_tcgen05_corrector_matches_mma_sync():
+    """The corrector's forward convolutions on tcgen05 (tensor memory
+    accumulators) give the same map as the mma.sync kernels, up to the
+    rounding of the BF16 activations between layers."""
+    x = fg.surrogate_receptor(21, 6000)
+    g = fg.Grid(45, 41, 37, 0.375)  # partial tiles on every axis
+    eps = fg.ddd_table()
+    ctx = fg.Context(0)
+    ctx.surrogate_load()
+    ctx.surrogate_set(probe_tol=0.0)
+    ctx.tune(fg.AG_TUNE_SURROGATE_TCGEN05, 0)
+    ref, _ = ctx.emap_surrogate(g, x, eps)
+    ctx.tune(fg.AG_TUNE_SURROGATE_TCGEN05, 1)
+    tc, _ = ctx.emap_surrogate(g, x, eps)
+    tc2, _ = ctx.emap_surrogate(g, x, eps)
+    ctx.close()
+    assert np.array_equal(tc, tc2)
+    assert np.max(np.abs(tc.astype(np.float64) - ref)) <= 2e-4
