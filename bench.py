@@ -7,7 +7,7 @@ the B200 engine.
 A step is one map set.  `value` is point-atom evaluations per second over all
 ranks (N_atoms x N_points per map set / map-set seconds), with the inputs
 resident in HBM; `e2e` is the same metric through the public C ABI with host
-buffers (upload, compute, download of all maps).  L2 is flushed (256 MiB
+buffers (ag_problem_compute: upload, compute, all maps back in host memory).  L2 is flushed (256 MiB
 write) between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
@@ -365,25 +365,22 @@ def main():
         emap_avg = sum(emap_ms) / len(emap_ms)
         aff_avg = ms_step - emap_avg
 
-        # ---- end to end through the C ABI with host buffers ----
-        out = torch.empty((nmaps + 2) * npts, dtype=torch.float32, pin_memory=True)
-        outp = out.numpy()
+        # ---- end to end through the whole-job C ABI call (ag_problem_compute):
+        # the parsed job's host arrays are uploaded, every map is computed and
+        # the map set is copied back to host memory, each step ----
         h2d = n_atoms * (32 + 4 + 4 + 4 + 4 + 48) + 8192 * 4
         h2d += prob.info.n_types * 801 * nmaps * 4
         d2h = (nmaps + 2) * npts * 4
         for _ in range(2):
-            ctx.upload(prob.grid, prob.receptor, prob.params, prob.inv_eps_ptr)
-            ctx.compute(fg.AG_WORK_ALL)
-            ctx.download(outp)
+            prob.compute(ctx)
         if dist:
             dist.barrier()
         e2e_t = []
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            ctx.upload(prob.grid, prob.receptor, prob.params, prob.inv_eps_ptr)
-            ctx.compute(fg.AG_WORK_ALL)
-            ctx.download(outp)
+            prob.compute(ctx)
             e2e_t.append(time.perf_counter() - t0)
+        outp = prob.maps().reshape(-1)
         e2e_s = max_over_ranks(sum(e2e_t) / len(e2e_t), dist, f"cuda:{local}")
         e2e_value = world * pairs / e2e_s
         check = float(np.abs(outp[nmaps * npts:(nmaps + 1) * npts]).max())

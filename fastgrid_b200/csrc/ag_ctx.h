@@ -102,6 +102,14 @@ struct ag_ctx {
   int checksumSplits = 0;
   double wSum = 0, wAbsSum = 0, lastChecksum = 0;
   agc::SurrState* surr = nullptr;
+  cudaStream_t copyStream = nullptr;  // device-to-host copies that overlap compute (whole-job path)
+  cudaEvent_t evAff = nullptr;
+  cudaError_t ensureCopyStream() {
+    if (copyStream) return cudaSuccess;
+    cudaError_t e = cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evAff, cudaEventDisableTiming);
+    return e;
+  }
   int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }
 };
 

@@ -132,6 +132,8 @@ struct Problem {
 
   // outputs: [numMaps atom maps][e][d], x fastest, FP32, unrounded
   std::vector<float> out;
+  const float* outView = nullptr;  // when set, the map set lives there (e.g. pinned memory) instead of `out`
+  const float* mapData() const { return outView ? outView : out.data(); }
   std::vector<float> floatingGrid;
 
   int numMaps() const { return (int)maps.size(); }

@@ -152,6 +152,8 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
                   &c->dAtoms, &c->donorMask, &c->closestH})
     b->release();
   if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->copyStream) cudaStreamDestroy(c->copyStream);
+  if (c->evAff) cudaEventDestroy(c->evAff);
   delete c;
   return AG_OK;
 }
@@ -741,6 +743,11 @@ struct ag_problem {
   ag::Log log;
   std::vector<int> mapHbond, mapIsHB, mapCov;
   std::vector<double> solparProbe, volProbe;
+  float* pinned = nullptr;  // page-locked host copy of the map set (the D2H copies land here)
+  size_t pinnedN = 0;
+  ~ag_problem() {
+    if (pinned) cudaFreeHost(pinned);
+  }
 };
 
 extern "C" int ag_problem_load(const char* gpf, int v4, const char* log_path, ag_problem** out) {
@@ -822,16 +829,38 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
   const double* eps = nullptr;
   ag_problem_views(P, &g, &r, &a, &eps);
   if (int e = ag_upload(c, &g, &r, &a, eps)) return e;
-  if (int e = ag_compute(c, AG_WORK_ALL)) return e;
   const int64_t np = c->npoints();
-  for (int m = 0; m < p.numMaps(); m++)
+  const int nm = p.numMaps();
+  // Affinity, d-map and covalent maps first; their copy to the host then runs
+  // on a second stream while the e-map (most of the time) is computed.
+  if (int e = ag_compute(c, AG_WORK_AFFINITY)) return e;
+  for (int m = 0; m < nm; m++)
     if (p.maps[m].isCovalent) {
       CK(agk::covalent_launch(c->maps.p + (size_t)m * np, g.nx, g.ny, g.nz, g.spacing, p.covalentPoint,
                               p.covHalfWidthSquaredInv, p.covBarrier, c->stream));
       c->launches++;
     }
-  p.out.resize((size_t)(p.numMaps() + 2) * np);
-  if (int e = ag_download(c, p.out.data())) return e;
+  const size_t total = (size_t)(nm + 2) * np;
+  if (P->pinnedN < total) {
+    if (P->pinned) cudaFreeHost(P->pinned);
+    P->pinned = nullptr;
+    P->pinnedN = 0;
+    CK(cudaHostAlloc((void**)&P->pinned, sizeof(float) * total, cudaHostAllocDefault));
+    P->pinnedN = total;
+  }
+  CK(c->ensureCopyStream());
+  CK(cudaEventRecord(c->evAff, c->stream));
+  CK(cudaStreamWaitEvent(c->copyStream, c->evAff, 0));
+  if (nm) CK(cudaMemcpyAsync(P->pinned, c->maps.p, sizeof(float) * nm * np, cudaMemcpyDeviceToHost, c->copyStream));
+  CK(cudaMemcpyAsync(P->pinned + (size_t)(nm + 1) * np, c->maps.p + (size_t)(nm + 1) * np, sizeof(float) * np,
+                     cudaMemcpyDeviceToHost, c->copyStream));
+  if (int e = ag_compute(c, AG_WORK_EMAP)) return e;
+  CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->copyStream));
+  if (int e = checkStatus(c)) return e;
+  p.out.clear();
+  p.outView = P->pinned;
   if (p.hasFloatingGrid()) {
     DevBuf<float> fg;
     CK(fg.ensure(np));
@@ -845,7 +874,9 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
   return AG_OK;
 }
 
-extern "C" const float* ag_problem_maps(const ag_problem* P) { return P && !P->p.out.empty() ? P->p.out.data() : nullptr; }
+extern "C" const float* ag_problem_maps(const ag_problem* P) {
+  return P && (P->p.outView || !P->p.out.empty()) ? P->p.mapData() : nullptr;
+}
 
 // ---------------------------------------------------------------------------
 // Batches: persistent kernels over the work units of many jobs, one CUDA graph
@@ -1122,7 +1153,7 @@ extern "C" int ag_batch_free(ag_batch* b) {
 }
 
 extern "C" int ag_problem_write(ag_problem* P) {
-  if (!P || P->p.out.empty()) return fail(AG_E_INVALID, "no computed maps");
+  if (!P || (P->p.out.empty() && !P->p.outView)) return fail(AG_E_INVALID, "no computed maps");
   try {
     for (int m = 0; m < P->p.numMaps() + 2; m++) ag::writeMap(P->p, m, P->log);
     ag::writeFloatingGrid(P->p, P->log);
@@ -1271,7 +1302,7 @@ int runMain(int argc, char** argv) {
   for (int m = 0; m < P.p.numMaps() + 2; m++) {
     double mn = ag::kBig, mx = -ag::kBig;
     for (int64_t j = 0; j < np; j++) {
-      double v = ag::roundOutput(P.p.out[(size_t)m * np + j]);
+      double v = ag::roundOutput(P.p.mapData()[(size_t)m * np + j]);
       mn = std::min(mn, v);
       mx = std::max(mx, v);
     }

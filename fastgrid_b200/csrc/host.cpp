@@ -807,7 +807,7 @@ void writeMap(const Problem& p, int mapIndex, Log& log) {
   const int nm = p.numMaps();
   std::string fname = mapIndex < nm ? p.maps[mapIndex].filename : (mapIndex == nm ? p.elecFilename : p.desolvFilename);
   if (fname.empty()) return;
-  writeValuesFile(fname, mapHeader(p), p.out.data() + (size_t)mapIndex * p.numPoints, p.numPoints, log);
+  writeValuesFile(fname, mapHeader(p), p.mapData() + (size_t)mapIndex * p.numPoints, p.numPoints, log);
 }
 
 void writeFloatingGrid(const Problem& p, Log& log) {

@@ -18,7 +18,8 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(REPO, "tests", "golden")
 sys.path.insert(0, REPO)
 
-CASES = ["colagen2", "hsg1_sm", "synth_c0", "synth_const_diel", "synth_covalent", "synth_paramfile_v4"]
+CASES = ["colagen2", "hsg1_sm", "synth_c0", "synth_const_diel", "synth_covalent", "synth_paramfile_v4",
+         "synth_disorder_h"]
 
 # Tolerances (unrounded values against the FP64 oracle):
 #   electrostatics: 1e-4 kcal/mol/e absolute

@@ -110,6 +110,9 @@ SYNTH = {
                                edits={"+front": ["parameter_file AD4.1_bound.dat"],
                                       "+after_receptor": ["receptor_types A C HD N OA SA"]},
                                v4=True),
+    "synth_disorder_h": dict(gen=dict(n_atoms=700, semi_axes=(12, 11, 10), npts=24, seed=13,
+                                      ligand_types="A C HD N NA OA SA"),
+                             edits={"+": ["disorder_h"]}, v4=False),
 }
 
 
