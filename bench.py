@@ -19,7 +19,10 @@ At N=1 the line also carries two supplementary measurements:
     direct sum over every point;
   "batch": 64 receptors of 1,000-30,000 atoms on odd grids of 41^3-161^3
     points with 6 ligand maps each, computed as one batch (persistent kernels
-    replayed from one CUDA graph, autotuned e-map tiles).
+    replayed from one CUDA graph, autotuned e-map tiles);
+  "config0": the small configuration (2,000 atoms, 61^3, 6 maps), with FastGrid's
+    CPU build (all host threads) and AutoGrid 4.2.1 (one thread) timed on the same
+    job in the cpu_baseline object.
 
 --impl reference times FastGrid's own CPU path (oracle/_ref/fastgrid4, built
 from the reference sources, all host threads) on a bounded sample of the same
@@ -47,6 +50,8 @@ WORKLOAD = dict(n_atoms=20000, semi_axes=(45, 35, 30), npts=160, seed=2,
                 ligand_types="A C HD N NA OA SA S F Cl")
 SLAB_Z = 20          # CPU sample: npts 160 160 20 (161 x 161 x 21 points)
 REF_BIN = os.path.join(HERE, "oracle", "_ref", "fastgrid4")
+AG421_BIN = os.path.join(HERE, "oracle", "_ref", "autogrid4")
+C0 = dict(n_atoms=2000, semi_axes=(20, 20, 20), npts=60, seed=1)  # 61^3, ligands A C HD N OA SA
 SURR_SEEDS = list(range(900001, 900021))   # held out: training uses seeds 1000003 * s + i
 # DRAM bytes of one emap_kernel launch on this workload (ncu dram__bytes_read.sum +
 # dram__bytes_write.sum): profiles/emap_kernel_20k_161.md.
@@ -115,6 +120,57 @@ def surrogate_section(fg, torch, ctx, stream, flush, np):
             "method": "exact near field within 10 A + 1.5 A far-field grid, trilinear + 3-layer 32-channel "
                       "BF16 3D-conv corrector (shipped weights), residual probes with direct-sum fallback",
             "l2": "flushed before each timed map"}
+
+
+def config0_section(fg, torch, ctx, stream, tmp, steps):
+    """The small configuration (2,000 atoms, 61^3, 6 maps) on the GPU: device map-set time and the
+    whole-job call's wall time."""
+    d = os.path.join(tmp, "c0")
+    os.makedirs(d, exist_ok=True)
+    fg.synth_write(d, "c0", **C0)
+    old = os.getcwd()
+    os.chdir(d)
+    try:
+        p = fg.Problem("c0.gpf", log="c0.glg")
+    finally:
+        os.chdir(old)
+    pairs = p.info.n_atoms * p.npoints
+    ctx.upload(p.grid, p.receptor, p.params, p.inv_eps_ptr)
+    for _ in range(3):
+        ctx.compute(fg.AG_WORK_ALL)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for _ in range(steps):
+            ctx.compute(fg.AG_WORK_ALL)
+        ev[1].record(stream)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[1]) / steps
+    p.compute(ctx)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p.compute(ctx)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
+    return {"workload": "synthetic receptor 2000 atoms (20 A globule), 61^3 grid @0.375 A, ligand types "
+                        "A C HD N OA SA (6 maps + e + d)", "pairs": pairs, "map_set_ms": ms,
+            "value": pairs / (ms * 1e-3), "unit": UNIT, "e2e_ms": e2e_ms}, d
+
+
+def config0_cpu(d):
+    """FastGrid's CPU build (all host threads) and AutoGrid 4.2.1 (one thread) on the small configuration."""
+    out = {}
+    if os.path.exists(REF_BIN):
+        t0 = time.perf_counter()
+        secs, _ = fastgrid_cpu_run(d, os.path.join(d, "c0.gpf"))
+        out.update(fastgrid_cpu_map_set_s=secs, fastgrid_cpu_wall_s=time.perf_counter() - t0,
+                   fastgrid_cpu_threads=os.cpu_count())
+    if os.path.exists(AG421_BIN):
+        t0 = time.perf_counter()
+        r = subprocess.run([AG421_BIN, "-p", "c0.gpf", "-l", "ag421.glg"], cwd=d, capture_output=True, text=True)
+        if r.returncode == 0:
+            out.update(autogrid421_wall_s=time.perf_counter() - t0, autogrid421_threads=1)
+    return out
 
 
 def batch_section(fg, ctx, tmp, steps, np):
@@ -294,6 +350,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-config0", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -402,6 +459,15 @@ def main():
             surr = surrogate_section(fg, torch, ctx, stream, flush, np)
         if world == 1 and not args.no_batch:
             batch = batch_section(fg, ctx, tmp, args.steps, np)
+        c0 = c0dir = None
+        if world == 1 and not args.no_config0:
+            c0, c0dir = config0_section(fg, torch, ctx, stream, tmp, args.steps)
+        if cpu is not None and c0dir is not None:
+            cpu["config0"] = config0_cpu(c0dir)
+            if c0 is not None and "fastgrid_cpu_map_set_s" in cpu["config0"]:
+                c0["speedup_vs_fastgrid_cpu"] = cpu["config0"]["fastgrid_cpu_map_set_s"] / (c0["map_set_ms"] * 1e-3)
+            if c0 is not None and "autogrid421_wall_s" in cpu["config0"]:
+                c0["speedup_vs_autogrid421"] = cpu["config0"]["autogrid421_wall_s"] / (c0["e2e_ms"] * 1e-3)
         if rank == 0:
             line = {
                 "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -421,7 +487,7 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_s * 1e3},
                 "gpu_launches": launches, "clocks": ck, "cpu_baseline": cpu,
-                "emap_abs_max": check, "surrogate": surr, "batch": batch,
+                "emap_abs_max": check, "surrogate": surr, "batch": batch, "config0": c0,
             }
             print(json.dumps(line))
         ctx.close()
