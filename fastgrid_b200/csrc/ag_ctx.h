@@ -97,7 +97,7 @@ struct ag_ctx {
   float rNear = 11.0f;
   float delta = 2.0e-3f;
   int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
-  int ctasPerSm = 2;
+  int ctasPerSm = agk::kEmapCtasPerSm;
   agc::DevBuf<double> checksum;
   int checksumSplits = 0;
   double wSum = 0, wAbsSum = 0, lastChecksum = 0;

@@ -9,6 +9,7 @@ namespace agk {
 constexpr int kNX = 8;            // e-map: consecutive x points per thread
 constexpr int kEmapKahan = 0;
 constexpr int kEmapPlain = 1;
+constexpr int kEmapCtasPerSm = 3;  // e-map CTAs resident per SM (register bound 85)
 
 // A CTA's work in the e-map: items [item0, item0+nitems) of the item list and
 // the CTA's box: local origin (grid-centred frame, A) and half extents

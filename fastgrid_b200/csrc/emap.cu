@@ -396,7 +396,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
 }
 
 template <bool DDD, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) emap_kernel(const __grid_constant__ EmapParams P) {
+__global__ void __launch_bounds__(kThreads, kEmapCtasPerSm) emap_kernel(const __grid_constant__ EmapParams P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   EmapSmem& S = *reinterpret_cast<EmapSmem*>(smem_raw);
   emap_unit<DDD, MODE>(P, blockIdx.x % P.nblocks, blockIdx.x / P.nblocks, S);
@@ -405,7 +405,8 @@ __global__ void __launch_bounds__(kThreads, 2) emap_kernel(const __grid_constant
 // Persistent kernel over the work units of many jobs (a batch of receptors):
 // every CTA takes the next unit (job, CTA box) from an atomic counter until
 // none is left; the host orders units by decreasing cost.  Jobs run without
-// an atom split and with the distance-dependent dielectric.
+// an atom split and with the distance-dependent dielectric.  Two CTAs per SM:
+// at three the per-unit job parameters spill and the batch gains nothing.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 2)
     emap_batch_kernel(const EmapParams* __restrict__ jobs, const int2* __restrict__ units, int nunits, int* counter) {
@@ -436,7 +437,7 @@ cudaError_t emap_batch_launch(const EmapParams* jobs, const int2* units, int nun
 
 // Persistent direct e-map over a device-side list of CTA boxes.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, kEmapCtasPerSm)
     emap_list_kernel(const __grid_constant__ EmapParams P, const int* __restrict__ list, const int* __restrict__ count,
                      int* counter) {
   extern __shared__ __align__(128) unsigned char smem_raw[];

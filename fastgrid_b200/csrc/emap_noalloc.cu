@@ -216,7 +216,7 @@ extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d
   // partial-sum array's capacity.
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int want = 4 * sms;
+  const int want = 2 * agk::kEmapCtasPerSm * sms;
   int nsplit = 1;
   if (nblocks < want && n_atoms > 512) nsplit = std::min((want + nblocks - 1) / nblocks, (n_atoms + 255) / 256);
   while (nsplit > 1 && (int64_t)nsplit * np > kNaMaxPartial) nsplit--;

@@ -555,7 +555,7 @@ int runEmapSurrogate(ag_ctx* c, float* dOut) {
     P.items = S.dItems.p;
     P.blocks = S.dBlocks.p;
     P.nblocks = nb;
-    CK(agk::emap_list_launch(P, S.list.p, S.count.p, S.counter.p, std::min(nb, 2 * sms(c)), c->stream));
+    CK(agk::emap_list_launch(P, S.list.p, S.count.p, S.counter.p, std::min(nb, agk::kEmapCtasPerSm * sms(c)), c->stream));
     c->launches += 2;
     S.statsValid = true;
   }

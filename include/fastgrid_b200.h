@@ -92,7 +92,7 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
  * the stated tolerances for every allowed value. */
 #define AG_TUNE_EMAP_RNEAR 1          /* A, >= 8: atoms nearer the CTA box take the exact-bin path (default 11) */
 #define AG_TUNE_EMAP_ANALYTIC_EVERY 2 /* 0 or >= 2: every n-th mid atom evaluates 332/eps analytically (default 0) */
-#define AG_TUNE_EMAP_CTAS_PER_SM 3    /* 1..8: CTAs per SM the atom split aims for on small grids (default 2) */
+#define AG_TUNE_EMAP_CTAS_PER_SM 3    /* 1..8: CTAs per SM the atom split aims for on small grids (default 3) */
 #define AG_TUNE_EMAP_WARP_COMPACT 4   /* 0/1: each warp's work items form a compact box (default 1) */
 #define AG_TUNE_EMAP_TILE 5           /* TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 11616) */
 #define AG_TUNE_SURROGATE_TCGEN05 6   /* 0/1: surrogate corrector convolutions on tcgen05 (1, default) or mma.sync (0) */
