@@ -28,7 +28,7 @@ AG_WORK_EMAP_SURROGATE = 4
 SURROGATE_WEIGHTS = 35424
 DEFAULT_WEIGHTS = os.path.join(HERE, "surrogate_weights.bin")
 AG_EMAP_KAHAN, AG_EMAP_PLAIN = 0, 1
-AG_TUNE_EMAP_RNEAR, AG_TUNE_EMAP_ANALYTIC_EVERY, AG_TUNE_EMAP_CTAS_PER_SM = 1, 2, 3
+AG_TUNE_EMAP_RNEAR, AG_TUNE_EMAP_ANALYTIC_PAIRS, AG_TUNE_EMAP_CTAS_PER_SM = 1, 2, 3
 AG_TUNE_EMAP_WARP_COMPACT, AG_TUNE_EMAP_TILE, AG_TUNE_SURROGATE_TCGEN05 = 4, 5, 6
 TABLE_LEN = 8192
 

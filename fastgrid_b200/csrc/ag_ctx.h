@@ -67,9 +67,9 @@ struct ag_ctx {
   int itemsFor[3] = {0, 0, 0};
   double itemsH = 0;
   int itemsTile = 0;
-  int tile[3] = {1, 16, 16};  // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
-  bool warpCompact = true;    // e-map items in warp-compact order (see makeItems)
-  bool itemsCompact = false; // the order hItems was built with
+  int tile[3] = {2, 8, 16};   // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
+  int warpCompact = 2;        // e-map item order: 0 rows, 1 warp-compact, 2 warp-compact with x-interleaved lane pairs
+  int itemsCompact = -1;      // the order hItems was built with
   std::vector<double> epsHost;  // the staged 332/eps table (FP64), empty for the constant dielectric
   std::vector<double> atomsHost;  // host copy of the staged atoms (x, y, z, w)
   uint64_t atomsVersion = 0;      // bumped whenever new atoms are staged
@@ -96,7 +96,9 @@ struct ag_ctx {
   int emapMode = agk::kEmapKahan;
   float rNear = 11.0f;
   float delta = 2.0e-3f;
-  int anaEvery = 0;  // mid-list atoms using the analytic dielectric: none (measured fastest on B200)
+  int anaPairs = 0;  // of each thread's 4 point pairs, those evaluating mid atoms' dielectric analytically
+                     // (none: measured fastest on B200, the analytic pairs' ex2 and series cost more than the
+                     // table reads they replace)
   int ctasPerSm = agk::kEmapCtasPerSm;
   agc::DevBuf<double> checksum;
   int checksumSplits = 0;
@@ -117,7 +119,7 @@ namespace agc {
 
 int checkGrid(const ag_grid* g);
 // E-map work items and CTA boxes of a grid for a CTA tile shape.
-void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vector<int>& items,
+void makeItems(const ag_grid& g, const int tile[3], int warpCompact, std::vector<int>& items,
                std::vector<agk::EmapBlock>& blocks);
 // Stage the e-map inputs of a job (atoms, dielectric table, CTA boxes).
 int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, bool deviceInputs);

@@ -9,6 +9,7 @@ namespace agk {
 constexpr int kNX = 8;            // e-map: consecutive x points per thread
 constexpr int kEmapKahan = 0;
 constexpr int kEmapPlain = 1;
+constexpr int kItemInterleaved = 1 << 30;  // e-map item flag: x points shared alternately with the partner column
 constexpr int kEmapCtasPerSm = 3;  // e-map CTAs resident per SM (register bound 85)
 
 // A CTA's work in the e-map: items [item0, item0+nitems) of the item list and
@@ -35,9 +36,10 @@ struct EmapParams {
   const double* thr;              // thr[k]: least r^2 whose reference bin is >= k
   float rnear2;                   // (100 * rNear)^2
   float delta;                    // guard half-width around bin edges (units of 0.01 A)
-  int anaEvery;                   // every anaEvery-th mid atom of a tile takes the analytic path (0: none)
-  float negLambda2;               // -0.3153767175 / 100 / ln 2: E = 2^(negLambda2 * bin)
-  float poly[6];                  // invEps(bin) = sum_n poly[n] E^n for E <= 0.0121
+  int anaPairs;                   // of a thread's kNX/2 point pairs, how many evaluate mid atoms' bins analytically
+  float2 negBias2;                // -2^23, both halves: bin = f + negBias2
+  float2 negLambda2;              // -0.3153767175 / 100 / ln 2, both halves: E = 2^(negLambda2 * bin)
+  float2 poly2[6];                // invEps(bin) = sum_n poly2[n] E^n (both halves equal) for E <= 0.031
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1
   unsigned* status;

@@ -165,13 +165,13 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       if (!(v >= 8.0 && v <= 40.0)) return fail(AG_E_INVALID, "rNear must be in [8, 40] A");
       c->rNear = (float)v;
       return AG_OK;
-    case AG_TUNE_EMAP_ANALYTIC_EVERY:
-      if (!(v == 0.0 || (v >= 2.0 && v <= 64.0))) return fail(AG_E_INVALID, "analytic-every must be 0 or 2..64");
-      c->anaEvery = (int)v;
+    case AG_TUNE_EMAP_ANALYTIC_PAIRS:
+      if (!(v == 0.0 || v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "analytic point pairs must be 0, 1 or 2");
+      c->anaPairs = (int)v;
       return AG_OK;
     case AG_TUNE_EMAP_WARP_COMPACT:
-      if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "warp-compact item order must be 0 or 1");
-      c->warpCompact = v != 0.0;
+      if (!(v == 0.0 || v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "e-map item order must be 0, 1 or 2");
+      c->warpCompact = (int)v;
       return AG_OK;
     case AG_TUNE_EMAP_TILE: {
       const int t = (int)v, tx = t / 10000, ty = (t / 100) % 100, tz = t % 100;
@@ -213,10 +213,18 @@ int checkGrid(const ag_grid* g) {
 
 // Work items of the e-map (NX points of one row each), grouped into CTAs of
 // 256 items walking tiles of TX x TY x TZ items, with each CTA's box.
-// warpCompact: inside a tile, items go in blocks of TX x 4 x 4 (x fastest),
+// warpCompact >= 1: inside a tile, items go in blocks of TX x 4 x 4 (x fastest),
 // so each warp's 32 items form a compact box (for kernels that skip atoms
 // per warp); otherwise x, then y, then z.
-void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vector<int>& items,
+// warpCompact == 2 (TX even): the two items of each pair of x columns, held by
+// neighbouring lanes, are marked kItemInterleaved and split the pair's 2 NX
+// points between them alternately, so the points a warp visits at one step k
+// form a 2 x 4 x 4 block of neighbouring grid points instead of a 1 x 4 x 8
+// one with columns NX points apart.  Their distances to an atom then span
+// fewer table bins, and the table reads of a warp hit fewer distinct words in
+// one shared-memory bank.  A column whose partner is past the grid edge keeps
+// its own NX consecutive points.
+void makeItems(const ag_grid& g, const int tile[3], int warpCompact, std::vector<int>& items,
                std::vector<agk::EmapBlock>& blocks) {
   const int nxc = (g.nx + agk::kNX - 1) / agk::kNX;
   const int TX = tile[0], TY = tile[1], TZ = tile[2];
@@ -238,7 +246,10 @@ void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vecto
             for (int yb = ty; yb < ty + TY; yb += 4)
               for (int z = zb; z < std::min(g.nz, zb + 4); z++)
                 for (int y = yb; y < std::min(g.ny, yb + 4); y++)
-                  for (int x = tx; x < std::min(nxc, tx + TX); x++) items.push_back(x | (y << 8) | (z << 19));
+                  for (int x = tx; x < std::min(nxc, tx + TX); x++) {
+                    const bool il = warpCompact == 2 && TX % 2 == 0 && (x ^ 1) < nxc;
+                    items.push_back(x | (y << 8) | (z << 19) | (il ? agk::kItemInterleaved : 0));
+                  }
         } else {
           for (int z = tz; z < std::min(g.nz, tz + TZ); z++)
             for (int y = ty; y < std::min(g.ny, ty + TY); y++)
@@ -256,7 +267,7 @@ void makeItems(const ag_grid& g, const int tile[3], bool warpCompact, std::vecto
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int k = 0; k < b.nitems; k++) {
       int v = items[i0 + k];
-      int xc = v & 0xFF, y = (v >> 8) & 0x7FF, z = (v >> 19) & 0x7FF;
+      int xc = v & 0xFF, y = (v >> 8) & 0x7FF, z = (v >> 19) & 0x7FF;  // the pair's union is the same box
       int xa = xc * agk::kNX, xb = std::min(g.nx - 1, xa + agk::kNX - 1);
       double p[2][3] = {{(xa - n2x) * h, (y - n2y) * h, (z - n2z) * h}, {(xb - n2x) * h, (y - n2y) * h, (z - n2z) * h}};
       for (int q = 0; q < 2; q++)
@@ -358,14 +369,17 @@ int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P)
   {
     const double a = 7.7839, rho = 66.57180475 / 78.4, g0 = 332.0 / 78.4;
     double rp = 1.0;
-    P.poly[0] = (float)g0;
+    P.poly2[0] = make_float2((float)g0, (float)g0);
     for (int n = 1; n < 6; n++) {
       const double prev = rp;
       rp *= rho;
-      P.poly[n] = (float)(g0 * (rp + a * prev));
+      const float v = (float)(g0 * (rp + a * prev));
+      P.poly2[n] = make_float2(v, v);
     }
-    P.negLambda2 = (float)(-0.3153767175 / 100.0 / std::log(2.0));
-    P.anaEvery = c->anaEvery;
+    const float nl = (float)(-0.3153767175 / 100.0 / std::log(2.0));
+    P.negLambda2 = make_float2(nl, nl);
+    P.negBias2 = make_float2(-8388608.f, -8388608.f);
+    P.anaPairs = c->anaPairs;
   }
   P.out = dOut;
   P.status = c->status.p;

@@ -49,10 +49,9 @@ struct EmapSmem {
   double4 ring[2][kTile];         // 16 KB, TMA destination
   float4 nearA[kTile];            // local scaled x, y, z and 100*w
   float4 midA[kTile];             // mid atoms, table read
-  float4 midB[kTile];             // mid atoms, analytic bin value
   float4 farA[kTile];             // w pre-multiplied by invEps[8191]
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
-  int cnt[4][kThreads / 32];
+  int cnt[3][kThreads / 32];
   double wpart[kThreads / 32];
   int unit;                       // persistent batch kernel: the unit being processed
   uint64_t bar[2];
@@ -93,57 +92,95 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
+// Packed FP32 pairs: Blackwell issues one instruction for two lanes of FP32
+// arithmetic (add/mul/fma .f32x2), each half rounded exactly as the scalar
+// operation, so the pair loops below halve their FP32 instruction count
+// without changing a bit of the result.
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ float2 rsqrt2(float2 v) { return make_float2(rsqrt_approx(v.x), rsqrt_approx(v.y)); }
+
 // Mid-list atoms: bin by a round-down FMA, plain FP32 chunk sums.
-// ANALYTIC = false: the bin's value is read from the shared-memory table.
-// ANALYTIC = true: the same value is evaluated on the FMA and SFU pipes,
+// The bin's value is read from the shared-memory table for the first
+// kNX/2 - NA point pairs of the thread and evaluated on the FMA and SFU pipes
+// for the last NA pairs:
 //   invEps(bin) = 332 (1 + a E) / (78.4 - c E),  E = exp(-0.3153767175 bin / 100)
-//   (autogrid.h:233-239), as the series sum_n P.poly[n] E^n; mid atoms are
+//   (autogrid.h:233-239), as the series sum_n P.poly2[n] E^n; mid atoms are
 //   at least rNear (default 11 A) away, so E <= 0.031 and the truncation is
-//   below 1e-8 relative (1e-6 at the smallest allowed rNear, 8 A).  Running
-//   part of the atoms this way takes load off the
-//   shared-memory pipe, whose random-bank table reads limit the kernel.
+//   below 1e-8 relative (1e-6 at the smallest allowed rNear, 8 A).
+// The table reads' bank conflicts make shared-memory wavefronts the kernel's
+// limit; evaluating some pairs analytically in the same instruction stream
+// moves that work onto the SFU (ex2) and FMA pipes, which run in parallel.
 // CLAMP: the CTA's box is large enough that a bin can pass the table's end.
-template <int MODE, bool CLAMP, bool ANALYTIC>
+// gxn holds minus the thread's x coordinates, in pairs (x0, x1), (x2, x3), ...
+template <int MODE, bool CLAMP, int NA>
 __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint32_t tabBiased, int n,
-                                          const float (&gx)[kNX], float gy, float gz, float (&sum)[kNX],
+                                          const float2 (&gxn)[kNX / 2], float gy, float gz, float (&sum)[kNX],
                                           float (&cmp)[kNX], const EmapParams& P) {
   const float kBias = 8388608.f;
+  const float2 bias2 = dup2(kBias);
 #pragma unroll 1
   for (int j0 = 0; j0 < n; j0 += kChunk) {
-    float cs[kNX];
+    float2 cs[kNX / 2];
 #pragma unroll
-    for (int k = 0; k < kNX; k++) cs[k] = (MODE == kEmapKahan) ? 0.f : sum[k];
+    for (int k = 0; k < kNX / 2; k++)
+      cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : make_float2(sum[2 * k], sum[2 * k + 1]);
     const int j1 = min(n, j0 + kChunk);
-#pragma unroll 1
+    // Unrolled over atoms: the scheduler interleaves several atoms' rsqrt and
+    // table-read latencies (3 CTAs x 8 warps per SM alone do not hide them).
+#pragma unroll 8
     for (int j = j0; j < j1; j++) {
       const float4 a = list[j];
       const float dy = a.y - gy, dz = a.z - gz;
-      const float dyz2 = fmaf(dz, dz, dy * dy);
+      const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy));
+      const float2 ax = dup2(a.x), aw = dup2(a.w);
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        const float dx = a.x - gx[k];
-        const float r2 = fmaf(dx, dx, dyz2);
-        const float rs = rsqrt_approx(r2);
-        float f = __fmaf_rd(r2, rs, kBias);
-        if (CLAMP) f = fminf(f, kBias + (float)(kTabLen - 1));
-        float g;
-        if (ANALYTIC) {
-          const float E = ex2_approx((f - kBias) * P.negLambda2);
-          g = fmaf(E, fmaf(E, fmaf(E, fmaf(E, fmaf(E, P.poly[5], P.poly[4]), P.poly[3]), P.poly[2]), P.poly[1]),
-                   P.poly[0]);
-        } else {
-          g = lds_bin(tabBiased, f);
+      for (int k = 0; k < kNX / 2; k++) {
+        const float2 dx = __fadd2_rn(ax, gxn[k]);
+        const float2 r2 = __ffma2_rn(dx, dx, dyz2);
+        const float2 rs = rsqrt2(r2);
+        float2 f = __ffma2_rd(r2, rs, bias2);
+        if (CLAMP) {
+          f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
+          f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
         }
-        cs[k] = fmaf(a.w * rs, g, cs[k]);
+        float2 g;
+        if (k >= kNX / 2 - NA) {
+          const float2 arg = __fmul2_rn(__fadd2_rn(f, P.negBias2), P.negLambda2);
+          const float2 E = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
+          g = __ffma2_rn(E, P.poly2[5], P.poly2[4]);
+          g = __ffma2_rn(E, g, P.poly2[3]);
+          g = __ffma2_rn(E, g, P.poly2[2]);
+          g = __ffma2_rn(E, g, P.poly2[1]);
+          g = __ffma2_rn(E, g, P.poly2[0]);
+        } else {
+          g = make_float2(lds_bin(tabBiased, f.x), lds_bin(tabBiased, f.y));
+        }
+        cs[k] = __ffma2_rn(__fmul2_rn(aw, rs), g, cs[k]);
       }
     }
+    float c1[kNX];
+#pragma unroll
+    for (int k = 0; k < kNX / 2; k++) { c1[2 * k] = cs[k].x; c1[2 * k + 1] = cs[k].y; }
     if (MODE == kEmapKahan) {
-      add_chunk<MODE>(sum, cmp, cs);
+      add_chunk<MODE>(sum, cmp, c1);
     } else {
 #pragma unroll
-      for (int k = 0; k < kNX; k++) sum[k] = cs[k];
+      for (int k = 0; k < kNX; k++) sum[k] = c1[k];
     }
   }
+}
+
+template <int MODE, bool CLAMP>
+__device__ __forceinline__ void mid_atoms_any(const float4* __restrict__ list, uint32_t tabBiased, int n,
+                                              const float2 (&gxn)[kNX / 2], float gy, float gz, float (&sum)[kNX],
+                                              float (&cmp)[kNX], const EmapParams& P) {
+  if (P.anaPairs == 1)
+    mid_atoms<MODE, CLAMP, 1>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
+  else if (P.anaPairs == 2)
+    mid_atoms<MODE, CLAMP, 2>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
+  else
+    mid_atoms<MODE, CLAMP, 0>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
 }
 
 // One work unit: CTA box `blk` of job P against atom split `split`.  Called
@@ -159,14 +196,23 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
   // This thread's points, in the CTA-local frame scaled by 100.
   const bool active = tid < B.nitems;
   int xc = 0, iy = 0, iz = 0;
-  unpack_item(P.items[B.item0 + (active ? tid : 0)], xc, iy, iz);
+  const int item = P.items[B.item0 + (active ? tid : 0)];
+  unpack_item(item, xc, iy, iz);
+  // x of point k = xb + k * xs: NX consecutive points, or every other point of
+  // the 2 NX points of an interleaved column pair.
+  const bool il = (item & kItemInterleaved) != 0;
+  const int xb = il ? (xc >> 1) * (2 * kNX) + (xc & 1) : xc * kNX;
+  const int xs = il ? 2 : 1;
   const double h = P.h;
   float gx[kNX];
 #pragma unroll
   for (int k = 0; k < kNX; k++)
-    gx[k] = (float)(((double)(xc * kNX + k - P.n2x) * h - B.ox) * 100.0);
+    gx[k] = (float)(((double)(xb + k * xs - P.n2x) * h - B.ox) * 100.0);
   const float gy = (float)(((double)(iy - P.n2y) * h - B.oy) * 100.0);
   const float gz = (float)(((double)(iz - P.n2z) * h - B.oz) * 100.0);
+  float2 gxn[kNX / 2];
+#pragma unroll
+  for (int k = 0; k < kNX / 2; k++) gxn[k] = make_float2(-gx[2 * k], -gx[2 * k + 1]);
 
   if (DDD) {
     const float4* src = reinterpret_cast<const float4*>(P.table);
@@ -231,28 +277,24 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
                   dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
       const float d2 = dx * dx + dy * dy + dz * dz;
       cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? 1 : 2);
-      if (cls == 1 && P.anaEvery > 0 && tid % P.anaEvery == P.anaEvery - 1) cls = 3;
       if (cls == 2) loc.w *= gFar;
     }
     const unsigned b0 = __ballot_sync(0xffffffffu, cls == 0);
     const unsigned b1 = __ballot_sync(0xffffffffu, cls == 1);
     const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-    const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
     if (lane == 0) {
       S.cnt[0][warp] = __popc(b0);
       S.cnt[1][warp] = __popc(b1);
       S.cnt[2][warp] = __popc(b2);
-      S.cnt[3][warp] = __popc(b3);
     }
     __syncthreads();
-    int nNear = 0, nMid = 0, nFar = 0, nMidB = 0, off0 = 0, off1 = 0, off2 = 0, off3 = 0;
+    int nNear = 0, nMid = 0, nFar = 0, off0 = 0, off1 = 0, off2 = 0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) {
-      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; off3 = nMidB; }
+      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; }
       nNear += S.cnt[0][w];
       nMid += S.cnt[1][w];
       nFar += S.cnt[2][w];
-      nMidB += S.cnt[3][w];
     }
     const unsigned lt = (1u << lane) - 1u;
     if (cls == 0) {
@@ -263,45 +305,45 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       S.midA[off1 + __popc(b1 & lt)] = loc;
     } else if (cls == 2) {
       S.farA[off2 + __popc(b2 & lt)] = loc;
-    } else if (cls == 3) {
-      S.midB[off3 + __popc(b3 & lt)] = loc;
     }
     __syncthreads();
 
-    // Mid atoms: table read (list A) or analytic bin value (list B).
+    // Mid atoms: table read or analytic bin value.
     if (DDD) {
       const uint32_t tabBiased = smem_u32(S.tab) - 0x2C000000u;
-      if (B.clampMid) {
-        mid_atoms<MODE, true, false>(S.midA, tabBiased, nMid, gx, gy, gz, sum, cmp, P);
-        mid_atoms<MODE, true, true>(S.midB, tabBiased, nMidB, gx, gy, gz, sum, cmp, P);
-      } else {
-        mid_atoms<MODE, false, false>(S.midA, tabBiased, nMid, gx, gy, gz, sum, cmp, P);
-        mid_atoms<MODE, false, true>(S.midB, tabBiased, nMidB, gx, gy, gz, sum, cmp, P);
-      }
+      if (B.clampMid)
+        mid_atoms_any<MODE, true>(S.midA, tabBiased, nMid, gxn, gy, gz, sum, cmp, P);
+      else
+        mid_atoms_any<MODE, false>(S.midA, tabBiased, nMid, gxn, gy, gz, sum, cmp, P);
     }
 
     // Far atoms: saturated dielectric (or the constant dielectric), no table.
 #pragma unroll 1
     for (int j0 = 0; j0 < nFar; j0 += kChunk) {
-      float cs[kNX];
+      float2 cs[kNX / 2];
 #pragma unroll
-      for (int k = 0; k < kNX; k++) cs[k] = (MODE == kEmapKahan) ? 0.f : sum[k];
+      for (int k = 0; k < kNX / 2; k++)
+        cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : make_float2(sum[2 * k], sum[2 * k + 1]);
       const int j1 = min(nFar, j0 + kChunk);
-#pragma unroll 1
+#pragma unroll 8
       for (int j = j0; j < j1; j++) {
         const float4 a = S.farA[j];
         const float dy = a.y - gy, dz = a.z - gz;
-        const float dyz2 = fmaf(dz, dz, dy * dy);
+        const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy));
+        const float2 ax = dup2(a.x), aw = dup2(a.w);
 #pragma unroll
-        for (int k = 0; k < kNX; k++) {
-          const float dx = a.x - gx[k];
-          cs[k] = fmaf(a.w, rsqrt_approx(fmaf(dx, dx, dyz2)), cs[k]);
+        for (int k = 0; k < kNX / 2; k++) {
+          const float2 dx = __fadd2_rn(ax, gxn[k]);
+          cs[k] = __ffma2_rn(aw, rsqrt2(__ffma2_rn(dx, dx, dyz2)), cs[k]);
         }
       }
-      if (MODE == kEmapKahan) add_chunk<MODE>(sum, cmp, cs);
+      float c1[kNX];
+#pragma unroll
+      for (int k = 0; k < kNX / 2; k++) { c1[2 * k] = cs[k].x; c1[2 * k + 1] = cs[k].y; }
+      if (MODE == kEmapKahan) add_chunk<MODE>(sum, cmp, c1);
       else
 #pragma unroll
-        for (int k = 0; k < kNX; k++) sum[k] = cs[k];
+        for (int k = 0; k < kNX; k++) sum[k] = c1[k];
     }
 
     // Near atoms: clamp 1/r at 2 and decide bins near an edge exactly.
@@ -342,7 +384,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
             if (flags & (1u << k)) {
               // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
               const int kmid = min(__float_as_int(fT[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
-              const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
+              const double gx64 = __dmul_rn((double)(xb + k * xs - P.n2x), h);
               const double ddx = __dsub_rn(a64.x, gx64);
               const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
               idx[k] = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
@@ -385,7 +427,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
   const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;
 #pragma unroll
   for (int k = 0; k < kNX; k++) {
-    const int x = xc * kNX + k;
+    const int x = xb + k * xs;
     if (x >= P.nx) break;
     const double v = (MODE == kEmapKahan) ? (double)sum[k] - (double)cmp[k] : (double)sum[k];
     if (P.nsplit == 1)

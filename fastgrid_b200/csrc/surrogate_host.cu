@@ -230,13 +230,15 @@ uint32_t spread3(uint32_t v) {
   return v;
 }
 
-// Work items (warp-compact order) and the Morton-sorted atoms with the
-// bounding box of every 256-atom tile, for the staged job.
+// Work items (warp-compact order, CTA tiles of 1 x 16 x 16 items: the near-field
+// kernel's box shape) and the Morton-sorted atoms with the bounding box of
+// every 256-atom tile, for the staged job.
 int surrPrepare(ag_ctx* c, SurrState& S) {
   const ag_grid& g = c->grid;
-  const int key[4] = {g.nx, g.ny, g.nz, c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2]};
+  static const int kTile[3] = {1, 16, 16};
+  const int key[4] = {g.nx, g.ny, g.nz, kTile[0] * 10000 + kTile[1] * 100 + kTile[2]};
   if (memcmp(key, S.itemsKey, sizeof key) != 0 || S.itemsH != g.spacing) {
-    makeItems(g, c->tile, true, S.hItems, S.hBlocks);
+    makeItems(g, kTile, 1, S.hItems, S.hBlocks);
     CK(S.dItems.ensure(S.hItems.size()));
     CK(S.dBlocks.ensure(S.hBlocks.size()));
     CK(cudaMemcpyAsync(S.dItems.p, S.hItems.data(), sizeof(int) * S.hItems.size(), cudaMemcpyHostToDevice,

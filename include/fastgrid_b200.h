@@ -91,10 +91,11 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
  * --cuda-* switches played this role for its kernels).  Results stay within
  * the stated tolerances for every allowed value. */
 #define AG_TUNE_EMAP_RNEAR 1          /* A, >= 8: atoms nearer the CTA box take the exact-bin path (default 11) */
-#define AG_TUNE_EMAP_ANALYTIC_EVERY 2 /* 0 or >= 2: every n-th mid atom evaluates 332/eps analytically (default 0) */
+#define AG_TUNE_EMAP_ANALYTIC_PAIRS 2 /* 0..2: of each thread's 4 point pairs, how many evaluate 332/eps analytically for atoms beyond rNear instead of reading the table (default 0) */
 #define AG_TUNE_EMAP_CTAS_PER_SM 3    /* 1..8: CTAs per SM the atom split aims for on small grids (default 3) */
-#define AG_TUNE_EMAP_WARP_COMPACT 4   /* 0/1: each warp's work items form a compact box (default 1) */
-#define AG_TUNE_EMAP_TILE 5           /* TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 11616) */
+#define AG_TUNE_EMAP_WARP_COMPACT 4   /* e-map item order: 0 rows, 1 each warp's items form a compact box, 2 as 1 with
+                                         neighbouring lanes sharing a 16-point x span alternately (default 2) */
+#define AG_TUNE_EMAP_TILE 5           /* direct e-map: TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 20816) */
 #define AG_TUNE_SURROGATE_TCGEN05 6   /* 0/1: surrogate corrector convolutions on tcgen05 (1, default) or mma.sync (0) */
 int ag_ctx_tune(ag_ctx* ctx, int knob, double value);
 
