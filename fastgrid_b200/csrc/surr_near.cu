@@ -62,22 +62,33 @@ __device__ __forceinline__ int block_compact(bool flag, int* cnt, int& total) {
   return off + __popc(b & ((1u << lane) - 1u));
 }
 
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float lo_hi(const float2& v, int k) { return (k & 1) ? v.y : v.x; }
+
 // Sum the near batch into this thread's points: for each atom within rcut of
 // a point, w (min(1/r, 2) invEps[bin] - psi(r)); bins within P.delta of an
-// edge are decided exactly in FP64 from the atom's FP64 record.
-__device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& P, int n, const float (&gx)[kNX],
-                                           float gy, float gz, int xc, int iy, int iz, const float (&wlo)[3],
-                                           const float (&whi)[3], float (&sum)[kNX], float (&cmp)[kNX]) {
+// edge are decided exactly in FP64 from the atom's FP64 record.  The point
+// pairs (x0, x1), (x2, x3), ... go through Blackwell's packed FP32
+// instructions (add/mul/fma .f32x2, each half rounded as the scalar one).
+// gxn holds minus the thread's x coordinates in those pairs.
+__device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& P, int n,
+                                           const float2 (&gxn)[kNX / 2], float gy, float gz, int xc, int iy, int iz,
+                                           const float (&wlo)[3], const float (&whi)[3], float (&sum)[kNX],
+                                           float (&cmp)[kNX]) {
   const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
   const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
-  const float warpCut2 = P.rcut2 * 1.0001f;
+  const float2 bias2 = dup2(kBias), mone2 = dup2(-1.f), mhalf2 = dup2(-0.5f);
+  const float2 np0 = dup2(-P.psi[0]), np1 = dup2(-P.psi[1]), np2 = dup2(-P.psi[2]);
+  const float edge = 0.5f - P.delta;
+  const float rcut2 = P.rcut2;
+  const float warpCut2 = rcut2 * 1.0001f;
   const uint32_t tabBiased = smem_u32(S.tab) - 0x2C000000u;  // address(tab) - 4 * bits(2^23)
   const double h = P.h;
 #pragma unroll 1
   for (int j0 = 0; j0 < n; j0 += kChunk) {
-    float cs[kNX];
+    float2 cs[kNX / 2];
 #pragma unroll
-    for (int k = 0; k < kNX; k++) cs[k] = 0.f;
+    for (int k = 0; k < kNX / 2; k++) cs[k] = make_float2(0.f, 0.f);
     const int j1 = min(n, j0 + kChunk);
 #pragma unroll 1
     for (int j = j0; j < j1; j++) {
@@ -89,35 +100,39 @@ __device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& 
         if (fmaf(ex, ex, fmaf(ey, ey, ez * ez)) >= warpCut2) continue;
       }
       const float dy = a.y - gy, dz = a.z - gz;
-      const float dyz2 = fmaf(dz, dz, dy * dy);
-      float rsv[kNX], r2v[kNX], psi[kNX];
+      // The 1e-30 keeps r2 > 0 (an atom on a grid point) without a per-point max.
+      const float2 dyz2 = dup2(fmaf(dz, dz, fmaf(dy, dy, 1e-30f)));
+      const float2 ax = dup2(a.x);
+      float2 rs[kNX / 2], r2[kNX / 2], npsi[kNX / 2], fr5[kNX / 2];
       uint32_t bits[kNX];
-      unsigned flags = 0;
+      bool any = false;
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        const float dx = a.x - gx[k];
-        const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
-        const float rs = rsqrt_approx(r2);
-        rsv[k] = rs;
-        r2v[k] = r2;
-        psi[k] = fmaf(r2, fmaf(r2, P.psi[2], P.psi[1]), P.psi[0]);
-        float f = __fmaf_rd(r2, rs, kBias);
-        f = fminf(f, kBias + (float)(kTabLen - 1));
-        bits[k] = __float_as_uint(f);
-        const float fr = r2 * rs - (f - kBias);  // fraction of 100 r
-        if (r2 < P.rcut2 && fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
+      for (int k = 0; k < kNX / 2; k++) {
+        const float2 dx = __fadd2_rn(ax, gxn[k]);
+        r2[k] = __ffma2_rn(dx, dx, dyz2);
+        rs[k] = make_float2(rsqrt_approx(r2[k].x), rsqrt_approx(r2[k].y));
+        npsi[k] = __ffma2_rn(r2[k], __ffma2_rn(r2[k], np2, np1), np0);
+        float2 f = __ffma2_rd(r2[k], rs[k], bias2);
+        f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
+        f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
+        bits[2 * k] = __float_as_uint(f.x);
+        bits[2 * k + 1] = __float_as_uint(f.y);
+        // fraction of 100 r, minus one half: within delta of a bin edge <=> |fr5| > 0.5 - delta
+        fr5[k] = __fadd2_rn(__fadd2_rn(__fmul2_rn(r2[k], rs[k]), __ffma2_rn(f, mone2, bias2)), mhalf2);
+        any |= ((r2[k].x < rcut2) & (fabsf(fr5[k].x) > edge)) | ((r2[k].y < rcut2) & (fabsf(fr5[k].y) > edge));
       }
-      if (__any_sync(0xffffffffu, flags != 0)) {
-        if (flags) {
+      if (__any_sync(0xffffffffu, any)) {
+        if (any) {
           const double4 a64 = S.nearD[j];
           const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
           const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
           const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
 #pragma unroll
           for (int k = 0; k < kNX; k++) {
-            if (flags & (1u << k)) {
+            const float r2k = lo_hi(r2[k >> 1], k);
+            if (r2k < rcut2 && fabsf(lo_hi(fr5[k >> 1], k)) > edge) {
               // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
-              const int kmid = min(__float_as_int(r2v[k] * rsv[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
+              const int kmid = min(__float_as_int(r2k * lo_hi(rs[k >> 1], k) + 12582912.f) - 0x4B400000, kTabLen - 1);
               const double gx64 = __dmul_rn((double)(xc * kNX + k - P.n2x), h);
               const double ddx = __dsub_rn(a64.x, gx64);
               const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
@@ -128,16 +143,18 @@ __device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& 
         }
       }
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        float t;
-        asm("ld.shared.f32 %0, [%1];" : "=f"(t) : "r"(tabBiased + (bits[k] << 2)));
-        const float term = fmaf(-a.w, psi[k], (a.w * fminf(rsv[k], cap)) * t);
-        cs[k] += r2v[k] < P.rcut2 ? term : 0.f;
+      for (int k = 0; k < kNX / 2; k++) {
+        float2 t;
+        asm("ld.shared.f32 %0, [%1];" : "=f"(t.x) : "r"(tabBiased + (bits[2 * k] << 2)));
+        asm("ld.shared.f32 %0, [%1];" : "=f"(t.y) : "r"(tabBiased + (bits[2 * k + 1] << 2)));
+        const float2 c = make_float2(fminf(rs[k].x, cap), fminf(rs[k].y, cap));
+        const float2 wm = make_float2(r2[k].x < rcut2 ? a.w : 0.f, r2[k].y < rcut2 ? a.w : 0.f);
+        cs[k] = __ffma2_rn(wm, __ffma2_rn(c, t, npsi[k]), cs[k]);
       }
     }
 #pragma unroll
     for (int k = 0; k < kNX; k++) {
-      const float y = cs[k] - cmp[k];
+      const float y = lo_hi(cs[k >> 1], k) - cmp[k];
       const float s1 = sum[k] + y;
       cmp[k] = (s1 - sum[k]) - y;
       sum[k] = s1;
@@ -163,6 +180,9 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
   float gx[kNX];
 #pragma unroll
   for (int k = 0; k < kNX; k++) gx[k] = (float)(((double)(xc * kNX + k - P.n2x) * h - B.ox) * 100.0);
+  float2 gxn[kNX / 2];
+#pragma unroll
+  for (int k = 0; k < kNX / 2; k++) gxn[k] = make_float2(-gx[2 * k], -gx[2 * k + 1]);
   const float gy = (float)(((double)(iy - P.n2y) * h - B.oy) * 100.0);
   const float gz = (float)(((double)(iz - P.n2z) * h - B.oz) * 100.0);
   // The box of this warp's points.
@@ -258,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
       int nNear;
       const int pos = block_compact(near, S.cnt, nNear);  // ends with a barrier: the ring slot is read
       if (nBatch + nNear > kNearCap) {
-        near_batch(S, P, nBatch, gx, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
+        near_batch(S, P, nBatch, gxn, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
         __syncthreads();
         nBatch = 0;
       }
@@ -270,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 2) surr_near_kernel(const __grid_con
     }
   }
   __syncthreads();
-  near_batch(S, P, nBatch, gx, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
+  near_batch(S, P, nBatch, gxn, gy, gz, xc, iy, iz, wlo, whi, sum, cmp);
 
   if (!active) return;
   const int64_t row = ((int64_t)iz * P.ny + iy) * P.nx;

@@ -26,28 +26,45 @@ __device__ __forceinline__ float ex2f_approx(float x) {
 
 // ---------------------------------------------------------------------------
 // Coarse far field: F(node) = sum over all atoms of w psi(|node - atom|).
-// One node per thread, atoms streamed through shared memory in FP32
+// Two nodes per thread (node and node + 256 of the CTA's 512), evaluated with
+// Blackwell's packed FP32 instructions (add/mul/fma .f32x2, each half rounded
+// as the scalar instruction), atoms streamed through shared memory in FP32
 // (grid-centred coordinates), plain FP32 sums over 32-atom chunks added in
 // FP64.  Atoms are split across blockIdx.y; partials are summed in order.
 // ---------------------------------------------------------------------------
+constexpr int kCoarseNodes = 512;  // nodes per CTA (256 threads x 2)
+
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
 __global__ void __launch_bounds__(256) surr_coarse_kernel(const CoarseParams P) {
   __shared__ float4 sA[256];
   const int tid = threadIdx.x;
   const SurrGeom& G = P.G;
   const int64_t NN = (int64_t)G.N[0] * G.N[1] * G.N[2];
-  const int64_t node = (int64_t)blockIdx.x * 256 + tid;
-  float gx = 0.f, gy = 0.f, gz = 0.f;
-  if (node < NN) {
-    const int I = (int)(node % G.N[0]), J = (int)((node / G.N[0]) % G.N[1]), K = (int)(node / ((int64_t)G.N[0] * G.N[1]));
-    gx = (float)((double)((I - G.halo) * G.R - G.n2x) * G.h);
-    gy = (float)((double)((J - G.halo) * G.R - G.n2y) * G.h);
-    gz = (float)((double)((K - G.halo) * G.R - G.n2z) * G.h);
+  const int64_t node0 = (int64_t)blockIdx.x * kCoarseNodes + tid, node1 = node0 + 256;
+  float gc[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int64_t node = q ? node1 : node0;
+    if (node < NN) {
+      const int I = (int)(node % G.N[0]), J = (int)((node / G.N[0]) % G.N[1]),
+                K = (int)(node / ((int64_t)G.N[0] * G.N[1]));
+      gc[q][0] = (float)((double)((I - G.halo) * G.R - G.n2x) * G.h);
+      gc[q][1] = (float)((double)((J - G.halo) * G.R - G.n2y) * G.h);
+      gc[q][2] = (float)((double)((K - G.halo) * G.R - G.n2z) * G.h);
+    }
   }
+  // Minus the node coordinates, one pair per axis.
+  const float2 ngx = make_float2(-gc[0][0], -gc[1][0]), ngy = make_float2(-gc[0][1], -gc[1][1]),
+               ngz = make_float2(-gc[0][2], -gc[1][2]);
   const SplitKernel& S = P.K;
-  const float eShift = -S.negLambda2 * S.shift;
+  const float2 nl2 = dup2(S.negLambda2), eShift2 = dup2(-S.negLambda2 * S.shift);
+  const float2 pA = dup2(S.pA), pB = dup2(S.pB), pC = dup2(S.pC);
+  const float2 q0 = dup2(S.poly[0]), q1 = dup2(S.poly[1]), q2 = dup2(S.poly[2]), q3 = dup2(S.poly[3]),
+               q4 = dup2(S.poly[4]), q5 = dup2(S.poly[5]);
   const int split = blockIdx.y;
   const int a0 = split * P.chunk, a1 = min(P.n_atoms, a0 + P.chunk);
-  double acc = 0.0;
+  double acc0 = 0.0, acc1 = 0.0;
   for (int t0 = a0; t0 < a1; t0 += 256) {
     __syncthreads();
     if (t0 + tid < a1) {
@@ -59,26 +76,36 @@ __global__ void __launch_bounds__(256) surr_coarse_kernel(const CoarseParams P) 
 #pragma unroll 1
     for (int j0 = 0; j0 < nt; j0 += 32) {
       const int j1 = min(nt, j0 + 32);
-      float s = 0.f;
+      float2 s = make_float2(0.f, 0.f);
 #pragma unroll 4
       for (int j = j0; j < j1; j++) {
         const float4 a = sA[j];
-        const float dx = a.x - gx, dy = a.y - gy, dz = a.z - gz;
-        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float rs = rsqrt_approx(fmaxf(r2, 1e-12f));
+        const float2 dx = __fadd2_rn(dup2(a.x), ngx), dy = __fadd2_rn(dup2(a.y), ngy),
+                     dz = __fadd2_rn(dup2(a.z), ngz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        // r2 = 0 (an atom on the node) gives rsqrt = inf and a NaN tail below,
+        // but r2 < a2 there, so the select takes the inner polynomial.
+        const float2 rs = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
         // E = exp(-lambda (r - shift)); past the table's end (81.91 A) the
         // reference's value stays at bin 8191, which differs from this by < 1e-10.
-        const float E = ex2f_approx(fmaf(r2 * rs, S.negLambda2, eShift));
-        const float tau =
-            fmaf(E, fmaf(E, fmaf(E, fmaf(E, fmaf(E, S.poly[5], S.poly[4]), S.poly[3]), S.poly[2]), S.poly[1]),
-                 S.poly[0]);
-        const float inner = fmaf(r2, fmaf(r2, S.pC, S.pB), S.pA);
-        s = fmaf(a.w, r2 < S.a2 ? inner : tau * rs, s);
+        const float2 arg = __ffma2_rn(__fmul2_rn(r2, rs), nl2, eShift2);
+        const float2 E = make_float2(ex2f_approx(arg.x), ex2f_approx(arg.y));
+        float2 tau = __ffma2_rn(E, q5, q4);
+        tau = __ffma2_rn(E, tau, q3);
+        tau = __ffma2_rn(E, tau, q2);
+        tau = __ffma2_rn(E, tau, q1);
+        tau = __ffma2_rn(E, tau, q0);
+        const float2 inner = __ffma2_rn(r2, __ffma2_rn(r2, pC, pB), pA);
+        const float2 outer = __fmul2_rn(tau, rs);
+        const float2 psi = make_float2(r2.x < S.a2 ? inner.x : outer.x, r2.y < S.a2 ? inner.y : outer.y);
+        s = __ffma2_rn(dup2(a.w), psi, s);
       }
-      acc += (double)s;
+      acc0 += (double)s.x;
+      acc1 += (double)s.y;
     }
   }
-  if (node < NN) P.partial[(int64_t)split * NN + node] = acc;
+  if (node0 < NN) P.partial[(int64_t)split * NN + node0] = acc0;
+  if (node1 < NN) P.partial[(int64_t)split * NN + node1] = acc1;
 }
 
 __global__ void surr_coarse_reduce_kernel(const double* __restrict__ partial, int nsplit, int64_t n,
@@ -711,7 +738,7 @@ cudaError_t bwdw_go(const BwdwArgs& A, int sms, cudaStream_t st) {
 cudaError_t surr_coarse_launch(const CoarseParams& P, cudaStream_t st) {
   const int64_t NN = (int64_t)P.G.N[0] * P.G.N[1] * P.G.N[2];
   if (P.n_atoms <= 0) return cudaMemsetAsync(P.field, 0, sizeof(double) * NN, st);
-  dim3 grid((unsigned)((NN + 255) / 256), (unsigned)P.nsplit);
+  dim3 grid((unsigned)((NN + kCoarseNodes - 1) / kCoarseNodes), (unsigned)P.nsplit);
   surr_coarse_kernel<<<grid, 256, 0, st>>>(P);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;

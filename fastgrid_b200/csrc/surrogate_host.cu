@@ -326,7 +326,7 @@ int surrBase(ag_ctx* c, SurrState& S, float* dBase, uint4* dFeat, float sIn) {
   }
   // coarse far field
   const int64_t NN = (int64_t)G.N[0] * G.N[1] * G.N[2];
-  const int64_t nodeBlocks = (NN + 255) / 256;
+  const int64_t nodeBlocks = (NN + 511) / 512;  // surr_coarse_kernel: 512 nodes per CTA
   int nsplit = (int)std::max<int64_t>(1, (8 * (int64_t)sms(c) + nodeBlocks - 1) / nodeBlocks);
   nsplit = std::min(nsplit, std::max(1, (c->nAtoms + 255) / 256));
   int chunk = (c->nAtoms + nsplit - 1) / nsplit;
