@@ -141,9 +141,12 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
   float rcx = 0.f, rcy = 0.f, rcz = 0.f;
   if (ch >= 0) { rcx = P.rv[3 * ch]; rcy = P.rv[3 * ch + 1]; rcz = P.rv[3 * ch + 2]; }
 
-  float em[NMAX], mn[kMaxMinMax], mx[kMaxMinMax];
+  // Map sums in pairs (maps 2i, 2i+1): the table row's float4 halves add with
+  // one packed FP32x2 instruction each (add.f32x2, rounded as two scalar adds).
+  float2 em[NMAX / 2];
+  float mn[kMaxMinMax], mx[kMaxMinMax];
 #pragma unroll
-  for (int g = 0; g < NMAX; g++) em[g] = 0.f;
+  for (int g = 0; g < NMAX / 2; g++) em[g] = make_float2(0.f, 0.f);
 #pragma unroll
   for (int s = 0; s < kMaxMinMax; s++) { mn[s] = 999999.f; mx[s] = -999999.f; }
   unsigned mmFlag = 0;
@@ -273,7 +276,10 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
                 racc = ra;
                 if (a.idx != ch && ch >= 0) {
                   const float c = rcx * a.rv[0] + rcy * a.rv[1] + rcz * a.rv[2];
-                  Hramp = 0.5f - 0.5f * cosf(acosf_c(c) * (120.f / 90.f));
+                  // cos on the SFU (absolute error ~4e-7 on [0, pi]); cos(x) = cos(2 pi - x)
+                  // folds 4 theta / 3 in [0, 4 pi / 3] into [0, pi].
+                  const float xr = acosf_c(c) * (120.f / 90.f);
+                  Hramp = 0.5f - 0.5f * __cosf(fminf(xr, 6.28318531f - xr));
                 }
               }
             } else if (hb == A1) {
@@ -320,10 +326,8 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
             for (int g4 = 0; g4 < NMAX / 4; g4++) {
               if (4 * g4 >= P.nmaps) break;
               const float4 q = row4[g4];
-              em[4 * g4] += q.x;
-              em[4 * g4 + 1] += q.y;
-              em[4 * g4 + 2] += q.z;
-              em[4 * g4 + 3] += q.w;
+              em[2 * g4] = __fadd2_rn(em[2 * g4], make_float2(q.x, q.y));
+              em[2 * g4 + 1] = __fadd2_rn(em[2 * g4 + 1], make_float2(q.z, q.w));
             }
             continue;
           }
@@ -334,13 +338,14 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
             if ((g & 3) == 0) q4 = row4[g >> 2];
             const float pwi = (g & 3) == 0 ? q4.x : (g & 3) == 1 ? q4.y : (g & 3) == 2 ? q4.z : q4.w;
             const unsigned mode = (modes >> (2 * g)) & 3u;
+            float& emg = (g & 1) ? em[g >> 1].y : em[g >> 1].x;
             if (mode == 0u) {
-              em[g] += pwi;
+              emg += pwi;
             } else {
               const float rsph = fminf(fmaxf(pwi * 0.01f, 0.f), 1.f);
               if (mode == 1u) {
                 const float e = dis ? (P.tableH ? P.tableH[max(0, iR - 110) * nmPad + g] : 0.f) : pwi;
-                em[g] += e * Hramp * (racc + (1.f - racc) * rsph);
+                emg += e * Hramp * (racc + (1.f - racc) * rsph);
               } else {
                 const float f = (mode == 2u) ? racc : rdon;
                 const float v = pwi * (f + (1.f - f) * rsph);
@@ -462,7 +467,7 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
   for (int g = 0; g < NMAX; g++) {
     if (g >= P.nmaps) break;
     if (P.mapCov[g]) continue;
-    float e = em[g] + (P.solparProbe[g] * S1 + P.volProbe[g] * S2);
+    float e = ((g & 1) ? em[g >> 1].y : em[g >> 1].x) + (P.solparProbe[g] * S1 + P.volProbe[g] * S2);
     const int mslot = P.mapMinMaxSlot[g];
 #pragma unroll
     for (int s = 0; s < kMaxMinMax; s++)

@@ -63,16 +63,38 @@ __device__ __forceinline__ void unpack_item(int v, int& xc, int& y, int& z) {
   z = (v >> 19) & 0x7FF;
 }
 
+// Packed FP32 pairs: Blackwell issues one instruction for two lanes of FP32
+// arithmetic (add/mul/fma .f32x2), each half rounded exactly as the scalar
+// operation, so the pair loops below halve their FP32 instruction count
+// without changing a bit of the result.  A thread's kNX points are held as
+// the pairs (x0, x1), (x2, x3), ...
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ float2 rsqrt2(float2 v) { return make_float2(rsqrt_approx(v.x), rsqrt_approx(v.y)); }
+
+__device__ __forceinline__ float lo_hi(const float2& v, int k) { return (k & 1) ? v.y : v.x; }
+
+// One Kahan step on a pair, (x - c), (s + y), ((s1 - s) - y) each rounded once
+// as in the scalar form (a * -1 + b is exact before its single rounding).
+__device__ __forceinline__ void kahan2(float2& s, float2& c, float2 x) {
+  const float2 m1 = dup2(-1.f);
+  const float2 y = __ffma2_rn(c, m1, x);
+  const float2 s1 = __fadd2_rn(s, y);
+  c = __ffma2_rn(y, m1, __ffma2_rn(s, m1, s1));
+  s = s1;
+}
+
+// Fold a chunk's plain FP32 sums into the running sums (Kahan), or, in plain
+// mode, take them over (the chunk sums started from the running sums).
 template <int MODE>
-__device__ __forceinline__ void add_chunk(float (&sum)[kNX], float (&cmp)[kNX], const float (&cs)[kNX]) {
-  if (MODE == kEmapKahan) {
+__device__ __forceinline__ void add_chunk(float2 (&sum)[kNX / 2], float2 (&cmp)[kNX / 2],
+                                          const float2 (&cs)[kNX / 2]) {
 #pragma unroll
-    for (int k = 0; k < kNX; k++) {
-      const float y = cs[k] - cmp[k];
-      const float s1 = sum[k] + y;
-      cmp[k] = (s1 - sum[k]) - y;
-      sum[k] = s1;
-    }
+  for (int k = 0; k < kNX / 2; k++) {
+    if (MODE == kEmapKahan)
+      kahan2(sum[k], cmp[k], cs[k]);
+    else
+      sum[k] = cs[k];
   }
 }
 
@@ -92,14 +114,6 @@ __device__ __forceinline__ float ex2_approx(float x) {
   return y;
 }
 
-// Packed FP32 pairs: Blackwell issues one instruction for two lanes of FP32
-// arithmetic (add/mul/fma .f32x2), each half rounded exactly as the scalar
-// operation, so the pair loops below halve their FP32 instruction count
-// without changing a bit of the result.
-__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
-
-__device__ __forceinline__ float2 rsqrt2(float2 v) { return make_float2(rsqrt_approx(v.x), rsqrt_approx(v.y)); }
-
 // Mid-list atoms: bin by a round-down FMA, plain FP32 chunk sums.
 // The bin's value is read from the shared-memory table for the first
 // kNX/2 - NA point pairs of the thread and evaluated on the FMA and SFU pipes
@@ -115,8 +129,8 @@ __device__ __forceinline__ float2 rsqrt2(float2 v) { return make_float2(rsqrt_ap
 // gxn holds minus the thread's x coordinates, in pairs (x0, x1), (x2, x3), ...
 template <int MODE, bool CLAMP, int NA>
 __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint32_t tabBiased, int n,
-                                          const float2 (&gxn)[kNX / 2], float gy, float gz, float (&sum)[kNX],
-                                          float (&cmp)[kNX], const EmapParams& P) {
+                                          const float2 (&gxn)[kNX / 2], float gy, float gz, float2 (&sum)[kNX / 2],
+                                          float2 (&cmp)[kNX / 2], const EmapParams& P) {
   const float kBias = 8388608.f;
   const float2 bias2 = dup2(kBias);
 #pragma unroll 1
@@ -124,7 +138,7 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
     float2 cs[kNX / 2];
 #pragma unroll
     for (int k = 0; k < kNX / 2; k++)
-      cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : make_float2(sum[2 * k], sum[2 * k + 1]);
+      cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : sum[k];
     const int j1 = min(n, j0 + kChunk);
     // Unrolled over atoms: the scheduler interleaves several atoms' rsqrt and
     // table-read latencies (3 CTAs x 8 warps per SM alone do not hide them).
@@ -159,22 +173,14 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
         cs[k] = __ffma2_rn(__fmul2_rn(aw, rs), g, cs[k]);
       }
     }
-    float c1[kNX];
-#pragma unroll
-    for (int k = 0; k < kNX / 2; k++) { c1[2 * k] = cs[k].x; c1[2 * k + 1] = cs[k].y; }
-    if (MODE == kEmapKahan) {
-      add_chunk<MODE>(sum, cmp, c1);
-    } else {
-#pragma unroll
-      for (int k = 0; k < kNX; k++) sum[k] = c1[k];
-    }
+    add_chunk<MODE>(sum, cmp, cs);
   }
 }
 
 template <int MODE, bool CLAMP>
 __device__ __forceinline__ void mid_atoms_any(const float4* __restrict__ list, uint32_t tabBiased, int n,
-                                              const float2 (&gxn)[kNX / 2], float gy, float gz, float (&sum)[kNX],
-                                              float (&cmp)[kNX], const EmapParams& P) {
+                                              const float2 (&gxn)[kNX / 2], float gy, float gz, float2 (&sum)[kNX / 2],
+                                              float2 (&cmp)[kNX / 2], const EmapParams& P) {
   if (P.anaPairs == 1)
     mid_atoms<MODE, CLAMP, 1>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
   else if (P.anaPairs == 2)
@@ -232,10 +238,10 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     tma_load_1d(S.ring[0], P.atoms + a0, n0 * 32u, &S.bar[0]);
   }
 
-  float sum[kNX], cmp[kNX];
+  float2 sum[kNX / 2], cmp[kNX / 2];
   double wsum = 0.0;  // FP64 sum of the weights this thread converted (checksum)
 #pragma unroll
-  for (int k = 0; k < kNX; k++) { sum[k] = 0.f; cmp[k] = 0.f; }
+  for (int k = 0; k < kNX / 2; k++) { sum[k] = make_float2(0.f, 0.f); cmp[k] = make_float2(0.f, 0.f); }
 
   const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
   const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
@@ -323,7 +329,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       float2 cs[kNX / 2];
 #pragma unroll
       for (int k = 0; k < kNX / 2; k++)
-        cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : make_float2(sum[2 * k], sum[2 * k + 1]);
+        cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : sum[k];
       const int j1 = min(nFar, j0 + kChunk);
 #pragma unroll 8
       for (int j = j0; j < j1; j++) {
@@ -337,13 +343,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
           cs[k] = __ffma2_rn(aw, rsqrt2(__ffma2_rn(dx, dx, dyz2)), cs[k]);
         }
       }
-      float c1[kNX];
-#pragma unroll
-      for (int k = 0; k < kNX / 2; k++) { c1[2 * k] = cs[k].x; c1[2 * k + 1] = cs[k].y; }
-      if (MODE == kEmapKahan) add_chunk<MODE>(sum, cmp, c1);
-      else
-#pragma unroll
-        for (int k = 0; k < kNX; k++) sum[k] = c1[k];
+      add_chunk<MODE>(sum, cmp, cs);
     }
 
     // Near atoms: clamp 1/r at 2 and decide bins near an edge exactly.
@@ -351,59 +351,65 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     for (int j = 0; j < nNear; j++) {
       const float4 a = S.nearA[j];
       const float dy = a.y - gy, dz = a.z - gz;
-      const float dyz2 = fmaf(dz, dz, dy * dy);
-      float rsv[kNX];
-      float fT[kNX];  // 100 r (FP32), kept for the rare exact-bin fallback
-      int idx[kNX];
-      unsigned flags = 0;
+      // The 1e-30 keeps r2 > 0 (an atom on a grid point) without a per-point max.
+      const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy) + 1e-30f);
+      const float2 ax = dup2(a.x), aw = dup2(a.w);
+      float2 rsv[kNX / 2];
+      float2 fT[kNX / 2];   // 100 r (FP32), kept for the rare exact-bin fallback
+      float2 fr5[kNX / 2];  // fraction of 100 r minus one half
+      uint32_t bits[kNX];   // 2^23 + bin, as float bits
+      bool any = false;
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        const float dx = a.x - gx[k];
-        const float r2 = fmaxf(fmaf(dx, dx, dyz2), 1e-30f);
-        const float rs = rsqrt_approx(r2);
-        rsv[k] = rs;
+      for (int k = 0; k < kNX / 2; k++) {
+        const float2 dx = __fadd2_rn(ax, gxn[k]);
+        const float2 r2 = __ffma2_rn(dx, dx, dyz2);
+        rsv[k] = rsqrt2(r2);
         if (DDD) {
-          const float T = r2 * rs;
-          fT[k] = T;
-          float f = __fmaf_rd(r2, rs, kBias);
-          f = fminf(f, kBias + (float)(kTabLen - 1));
-          idx[k] = __float_as_int(f) - 0x4B000000;
+          fT[k] = __fmul2_rn(r2, rsv[k]);
+          float2 f = __ffma2_rd(r2, rsv[k], dup2(kBias));
+          f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
+          f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
+          bits[2 * k] = __float_as_uint(f.x);
+          bits[2 * k + 1] = __float_as_uint(f.y);
           // Within delta of a bin edge <=> the fraction of T is within delta of 0 or 1.
-          const float fr = T - (f - kBias);
-          if (fabsf(fr - 0.5f) > 0.5f - P.delta) flags |= 1u << k;
+          fr5[k] = __fadd2_rn(__fadd2_rn(fT[k], __ffma2_rn(f, dup2(-1.f), dup2(kBias))), dup2(-0.5f));
+          any |= (fabsf(fr5[k].x) > 0.5f - P.delta) | (fabsf(fr5[k].y) > 0.5f - P.delta);
         }
       }
-      if (DDD && __any_sync(0xffffffffu, flags != 0)) {
-        if (flags) {
+      if (DDD && __any_sync(0xffffffffu, any)) {
+        if (any) {
           const double4 a64 = S.ring[slot][S.nearIdx[j]];
           const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
           const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
           const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
 #pragma unroll
           for (int k = 0; k < kNX; k++) {
-            if (flags & (1u << k)) {
+            if (fabsf(lo_hi(fr5[k >> 1], k)) > 0.5f - P.delta) {
               // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
-              const int kmid = min(__float_as_int(fT[k] + 12582912.f) - 0x4B400000, kTabLen - 1);
+              const int kmid = min(__float_as_int(lo_hi(fT[k >> 1], k) + 12582912.f) - 0x4B400000, kTabLen - 1);
               const double gx64 = __dmul_rn((double)(xb + k * xs - P.n2x), h);
               const double ddx = __dsub_rn(a64.x, gx64);
               const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
-              idx[k] = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
+              const int b = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
+              bits[k] = 0x4B000000u + (uint32_t)b;
             }
           }
         }
       }
+      const uint32_t tabB = smem_u32(S.tab) - 0x2C000000u;  // address(tab) - 4 * bits(2^23)
 #pragma unroll
-      for (int k = 0; k < kNX; k++) {
-        const float c = fminf(rsv[k], cap);
-        const float term = DDD ? (a.w * c) * S.tab[idx[k]] : a.w * c;
-        if (MODE == kEmapKahan) {
-          const float y = term - cmp[k];
-          const float s1 = sum[k] + y;
-          cmp[k] = (s1 - sum[k]) - y;
-          sum[k] = s1;
-        } else {
-          sum[k] += term;
+      for (int k = 0; k < kNX / 2; k++) {
+        float2 term = __fmul2_rn(aw, make_float2(fminf(rsv[k].x, cap), fminf(rsv[k].y, cap)));
+        if (DDD) {
+          float2 t;
+          asm("ld.shared.f32 %0, [%1];" : "=f"(t.x) : "r"(tabB + (bits[2 * k] << 2)));
+          asm("ld.shared.f32 %0, [%1];" : "=f"(t.y) : "r"(tabB + (bits[2 * k + 1] << 2)));
+          term = __fmul2_rn(term, t);
         }
+        if (MODE == kEmapKahan)
+          kahan2(sum[k], cmp[k], term);
+        else
+          sum[k] = __fadd2_rn(sum[k], term);
       }
     }
     __syncthreads();  // ring slot and atom lists are free again
@@ -429,7 +435,8 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
   for (int k = 0; k < kNX; k++) {
     const int x = xb + k * xs;
     if (x >= P.nx) break;
-    const double v = (MODE == kEmapKahan) ? (double)sum[k] - (double)cmp[k] : (double)sum[k];
+    const double v = (MODE == kEmapKahan) ? (double)lo_hi(sum[k >> 1], k) - (double)lo_hi(cmp[k >> 1], k)
+                                          : (double)lo_hi(sum[k >> 1], k);
     if (P.nsplit == 1)
       P.out[row + x] = (float)v;
     else

@@ -101,7 +101,7 @@ __device__ __forceinline__ void near_batch(const NearSmem& S, const EmapParams& 
       }
       const float dy = a.y - gy, dz = a.z - gz;
       // The 1e-30 keeps r2 > 0 (an atom on a grid point) without a per-point max.
-      const float2 dyz2 = dup2(fmaf(dz, dz, fmaf(dy, dy, 1e-30f)));
+      const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy) + 1e-30f);
       const float2 ax = dup2(a.x);
       float2 rs[kNX / 2], r2[kNX / 2], npsi[kNX / 2], fr5[kNX / 2];
       uint32_t bits[kNX];
