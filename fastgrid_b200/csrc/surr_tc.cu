@@ -292,17 +292,21 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         if (i >= 2 && !mbar_wait_bounded(&tempty[b], (unsigned)(((i >> 1) - 1) & 1), status)) break;
         if (!mbar_wait_bounded(&full[st], (unsigned)((i / kStages) & 1), status)) break;
         tc_fence_after();
-        const uint32_t aBase = sXa + (uint32_t)(st * SH::kStageBytes);
         const uint32_t dcol = tbase + (uint32_t)(b * SH::kBufCols);
+        // Descriptors of the stage's and the weights' first core matrices; a tap
+        // or K step only adds its byte offset / 16 to the start-address field
+        // (bits 0-13, no carry: shared addresses stay below 256 KB).
+        const uint64_t aDesc0 = smem_desc(sXa + (uint32_t)(st * SH::kStageBytes), kPlane, kTcHX * 16);
+        const uint64_t bDesc0 = smem_desc(sWa, NOUT * 16, 128);
 #pragma unroll
         for (int j = 0; j < SH::kMmas; j++) {
           const int t = j / (CINP / 16), hh = j % (CINP / 16);
           const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint32_t aAddr = aBase + (uint32_t)(2 * hh * kPlane + ((dz * kTcHY + dy) * kTcHX + dx) * 16);
-          const uint32_t bAddr = sWa + (uint32_t)((t * (CINP / 8) + 2 * hh) * NOUT * 16);
+          const uint32_t aOff = (uint32_t)(2 * hh * kPlane + ((dz * kTcHY + dy) * kTcHX + dx) * 16);
+          const uint32_t bOff = (uint32_t)((t * (CINP / 8) + 2 * hh) * NOUT * 16);
           // MMA j accumulates into accumulator j % kAcc; the first MMA of each overwrites it
-          tc_mma(dcol + (uint32_t)((j % SH::kAcc) * NOUT), smem_desc(aAddr, kPlane, kTcHX * 16),
-                 smem_desc(bAddr, NOUT * 16, 128), idesc, j >= SH::kAcc ? 1u : 0u);
+          tc_mma(dcol + (uint32_t)((j % SH::kAcc) * NOUT), aDesc0 + (aOff >> 4), bDesc0 + (bOff >> 4), idesc,
+                 j >= SH::kAcc ? 1u : 0u);
         }
         tc_commit(&empty[st]);  // the halo stage is free once these MMAs complete
         tc_commit(&tfull[b]);   // ... and the accumulator buffer holds the tile
