@@ -350,12 +350,12 @@ __device__ __forceinline__ void aff_unit(const AffParams& P, const int cta, unsi
                 const float f = (mode == 2u) ? racc : rdon;
                 const float v = pwi * (f + (1.f - f) * rsph);
                 const int mslot = P.mapMinMaxSlot[g];
-#pragma unroll
-                for (int s = 0; s < kMaxMinMax; s++)
-                  if (s == mslot) {
-                    mn[s] = fminf(mn[s], v);
-                    mx[s] = fmaxf(mx[s], v);
-                  }
+                switch (mslot) {  // uniform across the CTA
+                  case 0: mn[0] = fminf(mn[0], v); mx[0] = fmaxf(mx[0], v); break;
+                  case 1: mn[1] = fminf(mn[1], v); mx[1] = fmaxf(mx[1], v); break;
+                  case 2: mn[2] = fminf(mn[2], v); mx[2] = fmaxf(mx[2], v); break;
+                  default: mn[3] = fminf(mn[3], v); mx[3] = fmaxf(mx[3], v); break;
+                }
                 mmFlag |= 1u << mslot;
               }
             }
