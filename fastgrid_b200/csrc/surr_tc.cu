@@ -114,18 +114,7 @@ __device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&r)[1
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
-__device__ __forceinline__ void tmem_ld1_nowait(uint32_t taddr, uint32_t& r) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
-}
 __device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// One FP32 column of this thread's TMEM lane.
-__device__ __forceinline__ float tmem_ld1(uint32_t taddr) {
-  uint32_t r;
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-  return __uint_as_float(r);
-}
 
 // 4-D TMA tile load global -> shared (no multicast), completion on `bar`.
 __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
@@ -152,7 +141,7 @@ struct TcShape {
   static constexpr int kStages = (kSmemBudget - kWBytes - 128) / kStageBytes < 8 ? (kSmemBudget - kWBytes - 128) / kStageBytes : 8;
   static constexpr int kAcc = 4;  // independent accumulators per tile (breaks the MMA dependency chain)
   static constexpr int kBufCols = kAcc * NOUT;
-  static constexpr int kTmemCols = 2 * kBufCols;  // two tile buffers: 256 (NOUT 32) or 128 (NOUT 16) columns
+  static constexpr int kTmemCols = 2 * kBufCols;  // two tile buffers: 256 columns
 };
 
 // Epilogue of one tile: the sum of its NACC accumulators (NOUT columns each,
@@ -166,19 +155,8 @@ __device__ __forceinline__ void tc_epilogue(const ConvArgs& A, uint32_t taddr, i
   const int x = x0 + (i & 7), y = y0 + (i >> 3);
   const bool inside = x < A.nx && y < A.ny;
   const int64_t p = ((int64_t)z0 * A.ny + y) * A.nx + x;
-  if (EPI == EPI_STORE || EPI == EPI_ADD) {  // output channel 0 only
-    uint32_t r[NACC];
-#pragma unroll
-    for (int a = 0; a < NACC; a++) tmem_ld1_nowait(rowAddr + (uint32_t)(a * NOUT), r[a]);  // every lane takes part
-    tmem_wait();
-    float o = 0.f;
-#pragma unroll
-    for (int a = 0; a < NACC; a++) o += __uint_as_float(r[a]);
-    o *= A.scale;
-    if (!inside) return;
-    if (EPI == EPI_STORE) A.outF[p] = o;
-    else A.outF[p] += o;
-  } else {
+  static_assert(EPI == EPI_LEAKY, "the 32-output layers write leaky-ReLU BF16 activations");
+  {
     const int64_t np = (int64_t)A.nx * A.ny * A.nz;
 #pragma unroll
     for (int hcol = 0; hcol < 2; hcol++) {  // channels 16 hcol .. 16 hcol + 15
@@ -215,7 +193,7 @@ __device__ __forceinline__ void tile_xyz(int tile, int ntx, int nty, int& x0, in
 
 // CIN: channels of the input tensor in global memory (8 or 32); CINP: channels
 // in the halo and K per tap (16 or 32, padding planes are zero); NOUT: MMA N
-// (32, or 16 for the one-output layer whose channel 0 is used).
+// (32).  The one-output layer has its own kernel, surr_conv_tc3_kernel.
 template <int CIN, int CINP, int NOUT, int EPI>
 __global__ void __launch_bounds__(kTcThreads, 1)
     surr_conv_tc_kernel(const __grid_constant__ CUtensorMap tmap, const ConvArgs A, const uint16_t* __restrict__ wtc,
@@ -333,13 +311,181 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(SH::kTmemCols));
 }
 
+// ---------------------------------------------------------------------------
+// Layer 3 (32 channels -> 1 output) as a GEMM over the taps.  With one output
+// channel, the layers' implicit GEMM would spend 27 x 2 MMAs of N 16 per tile
+// on one useful column, each re-reading 4 KB of activations.  Instead, for
+// every point h of the tile's halo,
+//
+//   Y[h][t] = sum_ci act[h][ci] W3[t][ci]      (M 128 halo points, N 32 = 27 taps + 5 zero, K 32),
+//
+// 5 x 2 MMAs per tile, and the epilogue gathers out(q) = sum_t Y[q + off(t)][t]
+// through shared memory (the halo point of a tap lives in another TMEM lane).
+// The halo planes are padded to 640 points so that the fifth M block stays
+// inside its plane; rows 540..639 hold stale data and their Y rows are unused.
+// ---------------------------------------------------------------------------
+constexpr int kT3Rows = 640;                          // 5 M blocks of 128 halo points
+constexpr int kT3Plane = kT3Rows * 16;                // bytes per 8-channel plane
+constexpr int kT3StageBytes = 4 * kT3Plane;           // 32 channels
+constexpr int kT3WBytes = 4 * 32 * 16;                // W[kchunk 4][tap 32][8 channels] BF16
+constexpr int kT3Stride = 27;                         // floats per halo point in the Y array (odd: no bank conflicts on writes)
+constexpr int kT3YBytes = kTcHalo * kT3Stride * 4;
+constexpr int kT3Stages0 = (kSmemBudget - kT3WBytes - kT3YBytes - 128) / kT3StageBytes;
+constexpr int kT3Stages = kT3Stages0 < 8 ? kT3Stages0 : 8;
+constexpr int kT3BufCols = 5 * 32;                    // one tile's Y in TMEM
+constexpr int kT3TmemCols = 512;                      // two tile buffers (320 columns), a power of two
+static_assert(kT3Stages >= 2, "layer-3 halo ring needs two stages");
+
+// The 128 epilogue threads (warps 0-3): named barrier 1, optionally or-reducing a flag.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ bool epi_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, 128, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    surr_conv_tc3_kernel(const __grid_constant__ CUtensorMap tmap, const ConvArgs A, const uint16_t* __restrict__ wtc,
+                         unsigned* status) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 128-byte aligned base (TMA destinations); the launch adds 128 bytes of slack.
+  unsigned char* smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  unsigned char* sW = smem;
+  unsigned char* sX = smem + kT3WBytes;
+  float* sY = reinterpret_cast<float*>(sX + kT3Stages * kT3StageBytes);
+  __shared__ uint64_t full[kT3Stages], empty[kT3Stages], tfull[2], tempty[2];
+  __shared__ uint32_t tmemBase;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntx = (A.nx + kTcX - 1) / kTcX, nty = (A.ny + kTcY - 1) / kTcY;
+  const int ntiles = ntx * nty * A.nz;
+  const int nmine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const uint32_t sXa = smem_u32(sX), sWa = smem_u32(sW);
+  constexpr uint32_t txBytes = 4u * (kTcHalo * 16);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmemBase)),
+                 "r"(kT3TmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+  }
+  if (tid == 0) {
+    for (int k = 0; k < kT3Stages; k++) {
+      mbar_init(&full[k], 1);
+      mbar_init(&empty[k], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
+    fence_barrier_init();
+  }
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(wtc);
+    uint4* dst = reinterpret_cast<uint4*>(sW);
+    for (int i = tid; i < kT3WBytes / 16; i += kTcThreads) dst[i] = __ldg(src + i);
+  }
+  fence_proxy_async();  // the weights written above are read by the tensor cores
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tmemBase;
+
+  if (warp == 5) {
+    // ---- TMA producer ----
+    if (lane == 0) {
+      for (int j = 0; j < nmine; j++) {
+        const int st = j % kT3Stages;
+        if (j >= kT3Stages && !mbar_wait_bounded(&empty[st], (unsigned)((j / kT3Stages - 1) & 1), status)) break;
+        int x0, y0, z0;
+        tile_xyz((int)blockIdx.x + j * (int)gridDim.x, ntx, nty, x0, y0, z0);
+        const uint32_t dst = sXa + (uint32_t)(st * kT3StageBytes);
+        mbar_arrive_expect_tx(&full[st], txBytes);
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+          tma_load_4d(dst + (uint32_t)(c * kT3Plane), &tmap, 8 * (x0 - 1), y0 - 1, z0 - 1, c, &full[st]);
+      }
+    }
+  } else if (warp == 4) {
+    // ---- MMA issuer: 5 M blocks x 2 K steps per tile ----
+    if (lane == 0) {
+      constexpr uint32_t idesc = instr_desc(32);
+      for (int i = 0; i < nmine; i++) {
+        const int st = i % kT3Stages, b = i & 1;
+        if (i >= 2 && !mbar_wait_bounded(&tempty[b], (unsigned)(((i >> 1) - 1) & 1), status)) break;
+        if (!mbar_wait_bounded(&full[st], (unsigned)((i / kT3Stages) & 1), status)) break;
+        tc_fence_after();
+        // Start-address field + offset / 16 (no carry: shared addresses stay below 256 KB).
+        const uint64_t aDesc0 = smem_desc(sXa + (uint32_t)(st * kT3StageBytes), kT3Plane, 128);
+        const uint64_t bDesc0 = smem_desc(sWa, 32 * 16, 128);
+#pragma unroll
+        for (int mb = 0; mb < 5; mb++)
+#pragma unroll
+          for (int hh = 0; hh < 2; hh++)
+            tc_mma(tbase + (uint32_t)(b * kT3BufCols + 32 * mb),
+                   aDesc0 + (uint64_t)((2 * hh * kT3Plane + mb * 128 * 16) >> 4),
+                   bDesc0 + (uint64_t)((2 * hh * 32 * 16) >> 4), idesc, hh ? 1u : 0u);
+        tc_commit(&empty[st]);
+        tc_commit(&tfull[b]);
+      }
+    }
+  } else {
+    // ---- epilogue warps 0-3 ----
+    const int q = 32 * warp + lane;        // output point of the tile: x = q & 7, y = q >> 3
+    const int hc = (q >> 3) * kTcHX + (q & 7);  // its halo index at tap (0, 0, 0)
+    for (int i = 0; i < nmine; i++) {
+      const int b = i & 1;
+      const bool ok = mbar_wait_bounded(&tfull[b], (unsigned)((i >> 1) & 1), status);
+      if (epi_any(!ok)) break;  // all four warps leave together
+      tc_fence_after();
+      // TMEM -> shared: lane 32 warp + lane of block mb is halo point 128 mb + 32 warp + lane.
+#pragma unroll 1
+      for (int mb = 0; mb < 5; mb++) {
+        float v[32];
+        tmem_ld32(tbase + (uint32_t)(b * kT3BufCols + 32 * mb) + ((uint32_t)(32 * warp) << 16), v);
+        const int h = 128 * mb + q;
+        if (h < kTcHalo) {
+#pragma unroll
+          for (int t = 0; t < 27; t++) sY[h * kT3Stride + t] = v[t];
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);  // the TMEM buffer is free again
+      epi_sync();                              // Y of the whole halo is in shared memory
+      int x0, y0, z0;
+      tile_xyz((int)blockIdx.x + i * (int)gridDim.x, ntx, nty, x0, y0, z0);
+      float o = 0.f;
+#pragma unroll
+      for (int t = 0; t < 27; t++) {
+        const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+        o += sY[(hc + (dz * kTcHY + dy) * kTcHX + dx) * kT3Stride + t];
+      }
+      o *= A.scale;
+      const int x = x0 + (q & 7), y = y0 + (q >> 3);
+      if (x < A.nx && y < A.ny) {
+        const int64_t p = ((int64_t)z0 * A.ny + y) * A.nx + x;
+        if (EPI == EPI_STORE) A.outF[p] = o;
+        else A.outF[p] += o;
+      }
+      epi_sync();  // every read of Y is done before the next tile overwrites it
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kT3TmemCols));
+}
+
 // Master FP32 weights -> the tcgen05 layouts of the three layers.
 __global__ void surr_pack_tc_kernel(const float* __restrict__ w, uint16_t* w1, uint16_t* w2, uint16_t* w3) {
   const float* W1 = w;
   const float* W2 = w + kSurrW1;
   const float* W3 = w + kSurrW1 + kSurrW2;
-  constexpr int n1 = TcShape<16, 32>::kWBytes / 2, n2 = TcShape<32, 32>::kWBytes / 2,
-                n3 = TcShape<32, 16>::kWBytes / 2;
+  constexpr int n1 = TcShape<16, 32>::kWBytes / 2, n2 = TcShape<32, 32>::kWBytes / 2, n3 = kT3WBytes / 2;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2 + n3; i += gridDim.x * blockDim.x) {
     // element i of a layout [kchunk][co][8]: k = 8 kchunk + (i % 8), co = (i / 8) % NOUT
     if (i < n1) {  // layer 1: CINP 16 (channels 8..15 zero), NOUT 32
@@ -348,9 +494,9 @@ __global__ void surr_pack_tc_kernel(const float* __restrict__ w, uint16_t* w1, u
     } else if (i < n1 + n2) {  // layer 2: CINP 32, NOUT 32
       const int j = i - n1, e = j % 8, co = (j / 8) % 32, kc = j / 256, k = 8 * kc + e, t = k / 32, ci = k % 32;
       w2[j] = __bfloat16_as_ushort(__float2bfloat16_rn(W2[(t * 32 + ci) * 32 + co]));
-    } else {  // layer 3: CINP 32, NOUT 16 (output channel 0 only)
-      const int j = i - n1 - n2, e = j % 8, co = (j / 8) % 16, kc = j / 128, k = 8 * kc + e, t = k / 32, ci = k % 32;
-      w3[j] = __bfloat16_as_ushort(__float2bfloat16_rn(co == 0 ? W3[t * 32 + ci] : 0.f));
+    } else {  // layer 3 as a GEMM over taps: [kchunk 4][tap 32][8 channels], taps 27..31 zero
+      const int j = i - n1 - n2, e = j % 8, t = (j / 8) % 32, kc = j / 256, ci = 8 * kc + e;
+      w3[j] = __bfloat16_as_ushort(__float2bfloat16_rn(t < 27 ? W3[t * 32 + ci] : 0.f));
     }
   }
 }
@@ -406,11 +552,25 @@ cudaError_t tc_go(const ConvArgs& A, const uint16_t* wtc, unsigned* status, int 
   return cudaGetLastError();
 }
 
+template <int EPI>
+cudaError_t tc3_go(const ConvArgs& A, const uint16_t* wtc, unsigned* status, int sms, cudaStream_t st) {
+  if ((reinterpret_cast<uintptr_t>(A.in) & 15) != 0) return cudaErrorInvalidValue;  // TMA base alignment
+  CUtensorMap map;
+  cudaError_t e = halo_map(&map, A.in, 32, A.nx, A.ny, A.nz);
+  if (e != cudaSuccess) return e;
+  const size_t smem = (size_t)kT3WBytes + (size_t)kT3Stages * kT3StageBytes + (size_t)kT3YBytes + 128;
+  e = cudaFuncSetAttribute(surr_conv_tc3_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int ntiles = ((A.nx + kTcX - 1) / kTcX) * ((A.ny + kTcY - 1) / kTcY) * A.nz;
+  const int grid = ntiles < sms ? ntiles : sms;  // one CTA per SM
+  surr_conv_tc3_kernel<EPI><<<grid, kTcThreads, smem, st>>>(map, A, wtc, status);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 size_t surr_tc_weight_elems(int layer) {
-  return layer == 1 ? TcShape<16, 32>::kWBytes / 2 : layer == 2 ? TcShape<32, 32>::kWBytes / 2
-                                                                : TcShape<32, 16>::kWBytes / 2;
+  return layer == 1 ? TcShape<16, 32>::kWBytes / 2 : layer == 2 ? TcShape<32, 32>::kWBytes / 2 : kT3WBytes / 2;
 }
 
 cudaError_t surr_pack_tc_launch(const float* w, uint16_t* w1, uint16_t* w2, uint16_t* w3, cudaStream_t st) {
@@ -422,8 +582,8 @@ cudaError_t surr_conv_tc_launch(int layer, int epi, const ConvArgs& A, const uin
                                 cudaStream_t st) {
   if (layer == 1 && epi == EPI_LEAKY) return tc_go<8, 16, 32, EPI_LEAKY>(A, wtc, status, sms, st);
   if (layer == 2 && epi == EPI_LEAKY) return tc_go<32, 32, 32, EPI_LEAKY>(A, wtc, status, sms, st);
-  if (layer == 3 && epi == EPI_ADD) return tc_go<32, 32, 16, EPI_ADD>(A, wtc, status, sms, st);
-  if (layer == 3 && epi == EPI_STORE) return tc_go<32, 32, 16, EPI_STORE>(A, wtc, status, sms, st);
+  if (layer == 3 && epi == EPI_ADD) return tc3_go<EPI_ADD>(A, wtc, status, sms, st);
+  if (layer == 3 && epi == EPI_STORE) return tc3_go<EPI_STORE>(A, wtc, status, sms, st);
   return cudaErrorInvalidValue;
 }
 
