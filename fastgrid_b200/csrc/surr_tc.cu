@@ -133,10 +133,14 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
 
 template <int CINP, int NOUT>
 struct TcShape {
-  static constexpr int kChunks = 27 * CINP / 8;        // 8-channel K chunks
-  static constexpr int kWBytes = kChunks * NOUT * 16;  // packed weights
+  // CINP 16 (8 real input channels): one K step of 16 covers two taps, the
+  // first tap's 8 channels and the next tap's 8, so the padding plane is not
+  // multiplied; the tap pairs (0,1), (2,3), ..., (24,25), (26, zero plane).
+  static constexpr bool kPairTaps = CINP == 16;
+  static constexpr int kChunks = kPairTaps ? 28 : 27 * CINP / 8;  // 8-channel K chunks
+  static constexpr int kWBytes = kChunks * NOUT * 16;              // packed weights
   static constexpr int kStageBytes = (CINP / 8) * kPlane;
-  static constexpr int kMmas = 27 * (CINP / 16);
+  static constexpr int kMmas = kPairTaps ? 14 : 27 * (CINP / 16);
   // halo tiles in flight: as many as the shared memory left after the weights holds, at most 8
   static constexpr int kStages = (kSmemBudget - kWBytes - 128) / kStageBytes < 8 ? (kSmemBudget - kWBytes - 128) / kStageBytes : 8;
   static constexpr int kAcc = 4;  // independent accumulators per tile (breaks the MMA dependency chain)
@@ -275,16 +279,30 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         // or K step only adds its byte offset / 16 to the start-address field
         // (bits 0-13, no carry: shared addresses stay below 256 KB).
         const uint64_t aDesc0 = smem_desc(sXa + (uint32_t)(st * SH::kStageBytes), kPlane, kTcHX * 16);
+        const uint64_t aDesc1 = smem_desc(sXa + (uint32_t)(st * SH::kStageBytes), 0, kTcHX * 16);  // LBO per MMA
         const uint64_t bDesc0 = smem_desc(sWa, NOUT * 16, 128);
 #pragma unroll
         for (int j = 0; j < SH::kMmas; j++) {
-          const int t = j / (CINP / 16), hh = j % (CINP / 16);
-          const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
-          const uint32_t aOff = (uint32_t)(2 * hh * kPlane + ((dz * kTcHY + dy) * kTcHX + dx) * 16);
-          const uint32_t bOff = (uint32_t)((t * (CINP / 8) + 2 * hh) * NOUT * 16);
+          uint64_t aDesc;
+          uint32_t bOff;
+          if constexpr (SH::kPairTaps) {
+            // K halves: tap 2j's window and tap 2j+1's window of plane 0, LBO bytes
+            // apart (the zero plane for the last, unpaired tap).
+            const int t = 2 * j, t2 = 2 * j + 1;
+            const uint32_t off1 = (uint32_t)((((t / 9) * kTcHY + (t / 3) % 3) * kTcHX + t % 3) * 16);
+            const uint32_t off2 = t2 < 27 ? (uint32_t)((((t2 / 9) * kTcHY + (t2 / 3) % 3) * kTcHX + t2 % 3) * 16)
+                                          : off1 + (uint32_t)kPlane;
+            aDesc = aDesc1 + (off1 >> 4) + ((uint64_t)((off2 - off1) >> 4) << 16);
+            bOff = (uint32_t)(2 * j * NOUT * 16);
+          } else {
+            const int t = j / (CINP / 16), hh = j % (CINP / 16);
+            const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+            const uint32_t aOff = (uint32_t)(2 * hh * kPlane + ((dz * kTcHY + dy) * kTcHX + dx) * 16);
+            aDesc = aDesc0 + (aOff >> 4);
+            bOff = (uint32_t)((t * (CINP / 8) + 2 * hh) * NOUT * 16);
+          }
           // MMA j accumulates into accumulator j % kAcc; the first MMA of each overwrites it
-          tc_mma(dcol + (uint32_t)((j % SH::kAcc) * NOUT), aDesc0 + (aOff >> 4), bDesc0 + (bOff >> 4), idesc,
-                 j >= SH::kAcc ? 1u : 0u);
+          tc_mma(dcol + (uint32_t)((j % SH::kAcc) * NOUT), aDesc, bDesc0 + (bOff >> 4), idesc, j >= SH::kAcc ? 1u : 0u);
         }
         tc_commit(&empty[st]);  // the halo stage is free once these MMAs complete
         tc_commit(&tfull[b]);   // ... and the accumulator buffer holds the tile
@@ -488,9 +506,9 @@ __global__ void surr_pack_tc_kernel(const float* __restrict__ w, uint16_t* w1, u
   constexpr int n1 = TcShape<16, 32>::kWBytes / 2, n2 = TcShape<32, 32>::kWBytes / 2, n3 = kT3WBytes / 2;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1 + n2 + n3; i += gridDim.x * blockDim.x) {
     // element i of a layout [kchunk][co][8]: k = 8 kchunk + (i % 8), co = (i / 8) % NOUT
-    if (i < n1) {  // layer 1: CINP 16 (channels 8..15 zero), NOUT 32
-      const int e = i % 8, co = (i / 8) % 32, kc = i / 256, k = 8 * kc + e, t = k / 16, ci = k % 16;
-      w1[i] = __bfloat16_as_ushort(__float2bfloat16_rn(ci < 8 ? W1[(t * 8 + ci) * 32 + co] : 0.f));
+    if (i < n1) {  // layer 1: [tap 28][co 32][8 channels], tap 27 zero (the unpaired last K half)
+      const int ci = i % 8, co = (i / 8) % 32, t = i / 256;
+      w1[i] = __bfloat16_as_ushort(__float2bfloat16_rn(t < 27 ? W1[(t * 8 + ci) * 32 + co] : 0.f));
     } else if (i < n1 + n2) {  // layer 2: CINP 32, NOUT 32
       const int j = i - n1, e = j % 8, co = (j / 8) % 32, kc = j / 256, k = 8 * kc + e, t = k / 32, ci = k % 32;
       w2[j] = __bfloat16_as_ushort(__float2bfloat16_rn(W2[(t * 32 + ci) * 32 + co]));
