@@ -93,6 +93,39 @@ def test_emap_edge_cases(ctx):
         assert np.abs(got - ref).max() <= E_TOL * max(1.0, np.abs(ref).max() * 1e-3)
 
 
+@pytest.mark.parametrize("order,tile,ana", [(0, 11616, 0), (1, 11616, 0), (2, 20816, 0), (2, 21608, 0),
+                                            (2, 40808, 0), (1, 20816, 1), (2, 20816, 2)])
+def test_emap_item_orders_tiles_and_analytic_pairs(order, tile, ana):
+    """Every e-map item order (rows, warp-compact, x-interleaved lane pairs),
+    several CTA tiles and the analytic-dielectric pairs against the oracle, on
+    grids whose x extent leaves partial and unpaired 8-point columns, with
+    atoms in the near, mid and far (saturated dielectric) classes."""
+    rng = np.random.default_rng(7)
+    eps = np.zeros(8192)
+    oracle.lib().oracle_ddd_table(oracle._dp(eps))
+    c = fg.Context(0)
+    try:
+        c.tune(fg.AG_TUNE_EMAP_WARP_COMPACT, order)
+        c.tune(fg.AG_TUNE_EMAP_TILE, tile)
+        c.tune(fg.AG_TUNE_EMAP_ANALYTIC_PAIRS, ana)
+        inner = rng.normal(0, 9.0, (2500, 3))
+        outer = rng.normal(0, 1.0, (60, 3))
+        outer = outer / np.linalg.norm(outer, axis=1, keepdims=True) * rng.uniform(55, 75, (60, 1))
+        pts = np.concatenate([inner, outer])
+        xyzw = np.concatenate([pts, rng.normal(0, 0.05, (len(pts), 1))], axis=1)
+        for (nx, ny, nz) in [(33, 45, 29), (45, 41, 37)]:
+            g = fg.Grid(nx, ny, nz, 0.375)
+            got = c.emap(g, xyzw, eps)
+            ref = oracle.emap(g, xyzw, eps)
+            assert np.abs(got - ref).max() <= E_TOL, (order, tile, ana, (nx, ny, nz), np.abs(got - ref).max())
+            if ana == 0:
+                got = c.emap(g, xyzw, None)
+                ref = oracle.emap(g, xyzw, None)
+                assert np.abs(got - ref).max() <= E_TOL * max(1.0, np.abs(ref).max() * 1e-3)
+    finally:
+        c.close()
+
+
 def test_large_config_sampled(tmp_path, ctx):
     """The large benchmark configuration (20,000 atoms, 161^3, 10 ligand maps)
     against the oracle on 1500 sampled points."""
