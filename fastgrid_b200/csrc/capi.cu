@@ -282,10 +282,12 @@ void makeItems(const ag_grid& g, const int tile[3], int warpCompact, std::vector
     b.hx = (float)(50.0 * (hi[0] - lo[0]) + 1.0);
     b.hy = (float)(50.0 * (hi[1] - lo[1]) + 1.0);
     b.hz = (float)(50.0 * (hi[2] - lo[2]) + 1.0);
-    // Atoms at least rFar from the box use the saturated dielectric; nearer ones
-    // read the table, whose index then stays below 8191 without clamping.
+    // Atoms at least rFar (50-55 A) from the box use the saturated dielectric
+    // (table entries past 55 A differ from entry 8191 by < 2.6e-7 relative, past
+    // 50 A by < 1.3e-6); nearer ones read the table, whose index then stays
+    // below 8191 without clamping.
     const double diag = 2.0 * std::sqrt((double)b.hx * b.hx + (double)b.hy * b.hy + (double)b.hz * b.hz) / 100.0;
-    const double rFar = std::max(50.0, std::min(60.0, 81.0 - diag));
+    const double rFar = std::max(50.0, std::min(55.0, 81.0 - diag));
     b.rfar2 = (float)((100.0 * rFar) * (100.0 * rFar));
     b.clampMid = rFar + diag >= 81.0 ? 1 : 0;  // mid-list bins may then exceed the table
     blocks.push_back(b);
