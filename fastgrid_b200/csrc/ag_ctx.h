@@ -42,6 +42,8 @@ struct DevBuf {
 };
 
 const std::vector<double>& binThresholds();
+// The same table written into thr[0 .. 8192], without allocating.
+void emapBinThresholdsInto(double* thr);
 const std::vector<double>& affinityBinThresholds();
 
 struct SurrState;                 // learned far-field surrogate (surrogate_host.cu)

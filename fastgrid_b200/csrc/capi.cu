@@ -38,26 +38,30 @@ int fail(int code, const char* fmt, ...) {
 // Threshold table for the exact e-map bin: thr[k] is the least double r^2
 // with int(sqrt(r^2) * 100.0) >= k under IEEE double rounding, i.e. the bin
 // the reference's FP64 code (Cpu.cpp:70-75) computes is k-1 below it and k
-// at or above it.
+// at or above it.  Fills thr[0 .. 8192] (found by bisection over doubles).
+void emapBinThresholdsInto(double* thr) {
+  thr[0] = 0.0;
+  for (int k = 1; k <= 8192; k++) {
+    double lo = 0.0, hi = (k / 100.0 + 1.0) * (k / 100.0 + 1.0);
+    uint64_t a, b;
+    memcpy(&a, &lo, 8);
+    memcpy(&b, &hi, 8);
+    while (b - a > 1) {
+      uint64_t m = a + (b - a) / 2;
+      double v;
+      memcpy(&v, &m, 8);
+      if (sqrt(v) * 100.0 >= (double)k) b = m; else a = m;
+    }
+    memcpy(&thr[k], &b, 8);
+  }
+}
+
 const std::vector<double>& binThresholds() {
   static std::vector<double> thr;
   static std::once_flag once;
   std::call_once(once, [] {
-    thr.assign(agk::kNX > 0 ? 8193 : 0, 0.0);
-    auto binOf = [](double r2) { return sqrt(r2) * 100.0; };
-    for (int k = 1; k <= 8192; k++) {
-      double lo = 0.0, hi = (k / 100.0 + 1.0) * (k / 100.0 + 1.0);
-      uint64_t a, b;
-      memcpy(&a, &lo, 8);
-      memcpy(&b, &hi, 8);
-      while (b - a > 1) {
-        uint64_t m = a + (b - a) / 2;
-        double v;
-        memcpy(&v, &m, 8);
-        if (binOf(v) >= (double)k) b = m; else a = m;
-      }
-      memcpy(&thr[k], &b, 8);
-    }
+    thr.assign(8193, 0.0);
+    emapBinThresholdsInto(thr.data());
   });
   return thr;
 }

@@ -11,20 +11,30 @@
 // Limits: at most kNaMaxItems = 1,048,576 work items of 8 x-points (about
 // 8.4 million grid points, e.g. 201^3), and the atom-split partial sums are
 // limited to kNaMaxPartial = 2,097,152 doubles (the split count is reduced to
-// fit).  Larger grids are rejected with AG_E_INVALID.  The arrays take about
+// fit).  Larger grids are rejected with AG_E_INVALID before any CUDA call, and
+// so are input pointers that are not 16-byte aligned (the kernel reads atoms
+// by 16-byte bulk copies and the table as float4).  The arrays take about
 // 21 MiB on every device that loads the library, until the process exits.
 //
 // Sharing: every call, from any thread or stream, uses the same device arrays,
 // and they keep the previous call's contents.  Calls whose GPU work overlaps
 // race on them; serialise such calls (same stream, or wait between them).
 // The per-device set-up (symbol addresses, the bin-threshold table) happens on
-// the first call on each device; make that first call before any stream
-// capture on the device.
+// the first call on each device, and again on the first call after the
+// device's context was re-created (e.g. after cudaDeviceReset); make that
+// first call before any stream capture on the device.  The call is
+// synchronous: it returns when its GPU work has finished.
+//
+// Net-charge checksum: the e-map kernel's first CTA of every atom split sums,
+// in FP64, the weights of the atoms that went through its tile ring; a
+// separate one-CTA kernel sums the input weights directly.  The call fails
+// with AG_E_DEVICE if the two differ (a lost or duplicated atom tile).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cuda.h>
 #include <mutex>
 
 #include "../../include/fastgrid_b200.h"
@@ -33,6 +43,9 @@
 namespace ag {
 void setLastError(const char* msg);  // capi.cu
 }
+namespace agc {
+void emapBinThresholdsInto(double* thr);  // capi.cu: fills thr[0 .. 8192], no allocation
+}
 
 namespace {
 
@@ -40,20 +53,26 @@ constexpr int kNaMaxItems = 1 << 20;             // 4 MiB of work items
 constexpr int kNaMaxBlocks = (kNaMaxItems + 255) / 256;
 constexpr int64_t kNaMaxPartial = 1 << 21;       // 16 MiB of FP64 partial sums
 constexpr int kNaThr = 8193;
+constexpr int kNaMaxSplit = 1024;                // atom splits (checksum slots)
 
 static __device__ __align__(256) double g_naPartial[kNaMaxPartial];
 static __device__ __align__(256) int g_naItems[kNaMaxItems];
 static __device__ __align__(256) agk::EmapBlock g_naBlocks[kNaMaxBlocks];
 static __device__ __align__(256) double g_naThr[kNaThr];
 static __device__ __align__(256) unsigned g_naStatus[64];
+static __device__ __align__(256) double g_naChecksum[kNaMaxSplit];
+static __device__ __align__(256) double g_naWeights[2];  // input sum w, sum |w|
 
 struct NaDevice {
   bool ready = false;
+  unsigned long long ctxId = 0;  // the context the set-up was done in
   double* partial = nullptr;
   int* items = nullptr;
   agk::EmapBlock* blocks = nullptr;
   double* thr = nullptr;
   unsigned* status = nullptr;
+  double* checksum = nullptr;
+  double* weights = nullptr;
 };
 
 constexpr int kNaMaxDevices = 64;
@@ -65,44 +84,89 @@ int g_hItems[kNaMaxItems];
 agk::EmapBlock g_hBlocks[kNaMaxBlocks];
 double g_hThr[kNaThr];
 bool g_thrReady = false;
+double g_hChecksum[kNaMaxSplit];
+double g_hWeights[2];
 
 int naFail(int code, const char* msg) {
   ag::setLastError(msg);  // read back with ag_last_error()
   return code;
 }
 
-// thr[k]: least double r^2 whose bin int(sqrt(r^2) * 100.0) is >= k.
+// thr[k]: least double r^2 whose bin int(sqrt(r^2) * 100.0) is >= k (the
+// table the ordinary e-map entry points use, written into the static array).
 void naThresholds() {
   if (g_thrReady) return;
-  g_hThr[0] = 0.0;
-  for (int k = 1; k < kNaThr; k++) {
-    double lo = 0.0, hi = (k / 100.0 + 1.0) * (k / 100.0 + 1.0);
-    uint64_t a, b;
-    memcpy(&a, &lo, 8);
-    memcpy(&b, &hi, 8);
-    while (b - a > 1) {
-      const uint64_t m = a + (b - a) / 2;
-      double v;
-      memcpy(&v, &m, 8);
-      if (sqrt(v) * 100.0 >= (double)k) b = m; else a = m;
-    }
-    memcpy(&g_hThr[k], &b, 8);
-  }
+  agc::emapBinThresholdsInto(g_hThr);
   g_thrReady = true;
 }
 
-int naSetup(int dev, NaDevice& d) {
-  if (d.ready) return AG_OK;
+// Unique id of the calling thread's current CUDA context, through the driver
+// entry points the runtime exposes (the library does not link libcuda).
+bool naContextId(unsigned long long& id) {
+  using GetCurrent = CUresult (*)(CUcontext*);
+  using GetId = CUresult (*)(CUcontext, unsigned long long*);
+  static GetCurrent getCurrent = nullptr;
+  static GetId getId = nullptr;
+  if (!getCurrent || !getId) {
+    void* a = nullptr;
+    void* b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b)
+      return false;
+    getCurrent = reinterpret_cast<GetCurrent>(a);
+    getId = reinterpret_cast<GetId>(b);
+  }
+  CUcontext ctx = nullptr;
+  if (getCurrent(&ctx) != CUDA_SUCCESS || !ctx) return false;
+  return getId(ctx, &id) == CUDA_SUCCESS;
+}
+
+// Sum of the input weights (w of every atom) and of their magnitudes, in FP64,
+// by one CTA in a fixed order: the reference value of the net-charge checksum.
+__global__ void na_weight_sum_kernel(const double4* __restrict__ atoms, int n, double* out) {
+  __shared__ double s[2][256];
+  double w = 0.0, a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = atoms[i].w;
+    w += v;
+    a += fabs(v);
+  }
+  s[0][threadIdx.x] = w;
+  s[1][threadIdx.x] = a;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      s[0][threadIdx.x] += s[0][threadIdx.x + o];
+      s[1][threadIdx.x] += s[1][threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = s[0][0];
+    out[1] = s[1][0];
+  }
+}
+
+// Symbol addresses of the scratch arrays in the current context, and (once
+// per context) the bin-threshold table.
+int naSetup(NaDevice& d) {
   if (cudaGetSymbolAddress((void**)&d.partial, g_naPartial) != cudaSuccess ||
       cudaGetSymbolAddress((void**)&d.items, g_naItems) != cudaSuccess ||
       cudaGetSymbolAddress((void**)&d.blocks, g_naBlocks) != cudaSuccess ||
       cudaGetSymbolAddress((void**)&d.thr, g_naThr) != cudaSuccess ||
-      cudaGetSymbolAddress((void**)&d.status, g_naStatus) != cudaSuccess)
+      cudaGetSymbolAddress((void**)&d.status, g_naStatus) != cudaSuccess ||
+      cudaGetSymbolAddress((void**)&d.checksum, g_naChecksum) != cudaSuccess ||
+      cudaGetSymbolAddress((void**)&d.weights, g_naWeights) != cudaSuccess)
     return naFail(AG_E_CUDA, "cudaGetSymbolAddress failed for the no-allocation scratch arrays");
+  unsigned long long id = 0;
+  if (!naContextId(id)) return naFail(AG_E_CUDA, "cannot identify the current CUDA context");
+  if (d.ready && d.ctxId == id) return AG_OK;
   naThresholds();
   if (cudaMemcpy(d.thr, g_hThr, sizeof g_hThr, cudaMemcpyHostToDevice) != cudaSuccess)
     return naFail(AG_E_CUDA, "cannot initialise the bin threshold table");
-  (void)dev;
+  d.ctxId = id;
   d.ready = true;
   return AG_OK;
 }
@@ -167,17 +231,24 @@ int naItems(const ag_grid& g, int& nitems) {
 
 extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps,
                                float* d_out, void* stream) {
+  // Every argument check comes before the first CUDA call: a rejected call
+  // touches no device.
   if (!grid || !d_out || n_atoms < 0 || (n_atoms > 0 && !d_xyzw))
     return naFail(AG_E_INVALID, "null argument or negative atom count");
   if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || grid->nx > 1025 || grid->ny > 1025 || grid->nz > 1025 ||
       !(grid->spacing > 0))
     return naFail(AG_E_INVALID, "grid outside 1..1025 points per axis or bad spacing");
+  if ((int64_t)((grid->nx + agk::kNX - 1) / agk::kNX) * grid->ny * grid->nz > kNaMaxItems)
+    return naFail(AG_E_INVALID, "grid too large for ag_emap_noalloc (more than 1048576 work items of 8 points)");
+  if ((reinterpret_cast<uintptr_t>(d_xyzw) & 15u) || (reinterpret_cast<uintptr_t>(d_inv_eps) & 15u))
+    return naFail(AG_E_INVALID, "d_xyzw and d_inv_eps must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(d_out) & 3u) return naFail(AG_E_INVALID, "d_out must be 4-byte aligned");
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices)
     return naFail(AG_E_CUDA, "no current CUDA device");
   std::lock_guard<std::mutex> lock(g_mu);
   NaDevice& D = g_dev[dev];
-  if (int e = naSetup(dev, D)) return e;
+  if (int e = naSetup(D)) return e;
   cudaStream_t st = (cudaStream_t)stream;
   int nitems = 0;
   const int nblocks = naItems(*grid, nitems);
@@ -185,13 +256,28 @@ extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d
     return naFail(AG_E_INVALID, "grid too large for ag_emap_noalloc (more than 1048576 work items of 8 points)");
   const int64_t np = (int64_t)grid->nx * grid->ny * grid->nz;
   if (n_atoms == 0) {
-    if (cudaMemsetAsync(d_out, 0, sizeof(float) * np, st) != cudaSuccess) return naFail(AG_E_CUDA, "memset failed");
+    if (cudaMemsetAsync(d_out, 0, sizeof(float) * np, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return naFail(AG_E_CUDA, "memset failed");
     return AG_OK;
   }
+  // Split atoms across CTAs when the grid alone cannot fill the GPU, within the
+  // partial-sum array's and the checksum array's capacity.
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int want = 2 * agk::kEmapCtasPerSm * sms;
+  int nsplit = 1;
+  if (nblocks < want && n_atoms > 512) nsplit = std::min((want + nblocks - 1) / nblocks, (n_atoms + 255) / 256);
+  nsplit = std::min(nsplit, kNaMaxSplit);
+  while (nsplit > 1 && (int64_t)nsplit * np > kNaMaxPartial) nsplit--;
+  const int chunk = ((n_atoms + nsplit - 1) / nsplit + 255) / 256 * 256;
+  nsplit = std::max(1, (n_atoms + chunk - 1) / chunk);
+
   if (cudaMemcpyAsync(D.items, g_hItems, sizeof(int) * nitems, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(D.blocks, g_hBlocks, sizeof(agk::EmapBlock) * nblocks, cudaMemcpyHostToDevice, st) !=
           cudaSuccess ||
-      cudaMemsetAsync(D.status, 0, sizeof(unsigned), st) != cudaSuccess)
+      cudaMemsetAsync(D.status, 0, sizeof(unsigned), st) != cudaSuccess ||
+      cudaMemsetAsync(D.checksum, 0xFF, sizeof(double) * nsplit, st) != cudaSuccess)  // NaN until written
     return naFail(AG_E_CUDA, "cannot stage the work list");
   // The host staging arrays are reused by the next call: wait for the copies.
   if (cudaStreamSynchronize(st) != cudaSuccess) return naFail(AG_E_CUDA, "stream error");
@@ -212,25 +298,24 @@ extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d
   P.delta = 2.0e-3f;
   P.out = d_out;
   P.status = D.status;
-  // Split atoms across CTAs when the grid alone cannot fill the GPU, within the
-  // partial-sum array's capacity.
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int want = 2 * agk::kEmapCtasPerSm * sms;
-  int nsplit = 1;
-  if (nblocks < want && n_atoms > 512) nsplit = std::min((want + nblocks - 1) / nblocks, (n_atoms + 255) / 256);
-  while (nsplit > 1 && (int64_t)nsplit * np > kNaMaxPartial) nsplit--;
-  int chunk = ((n_atoms + nsplit - 1) / nsplit + 255) / 256 * 256;
-  nsplit = std::max(1, (n_atoms + chunk - 1) / chunk);
+  P.checksum = D.checksum;
   P.chunk = chunk;
   P.nsplit = nsplit;
   P.partial = nsplit > 1 ? D.partial : nullptr;
+  na_weight_sum_kernel<<<1, 256, 0, st>>>(P.atoms, n_atoms, D.weights);
+  if (cudaGetLastError() != cudaSuccess) return naFail(AG_E_CUDA, "weight-sum launch failed");
   if (agk::emap_launch(P, d_inv_eps != nullptr, agk::kEmapKahan, nblocks * nsplit, st) != cudaSuccess)
     return naFail(AG_E_CUDA, "e-map launch failed");
   unsigned status = 0;
   if (cudaMemcpyAsync(&status, D.status, sizeof(unsigned), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(g_hChecksum, D.checksum, sizeof(double) * nsplit, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(g_hWeights, D.weights, sizeof g_hWeights, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return naFail(AG_E_CUDA, "e-map kernel failed");
   if (status) return naFail(AG_E_DEVICE, "the e-map kernel reported an error status (bounded wait expired)");
+  double s = 0.0;
+  for (int k = 0; k < nsplit; k++) s += g_hChecksum[k];
+  if (!(std::fabs(s - g_hWeights[0]) <= 1e-9 * g_hWeights[1] + 1e-12))
+    return naFail(AG_E_DEVICE, "net-charge checksum mismatch: the e-map kernel did not consume every atom once");
   return AG_OK;
 }

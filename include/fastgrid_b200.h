@@ -204,15 +204,21 @@ int ag_main(int argc, char** argv);
  * manage the GPU's memory in their own pool or run under a fixed memory budget
  * where an allocation could synchronise the device or fail mid-run.  Inputs
  * and output are the caller's device buffers: d_xyzw (n_atoms x 4 doubles,
- * as for ag_emap), d_inv_eps (8192 FP32 values of 332/eps, or NULL for the
- * constant dielectric), d_out (nx*ny*nz floats); work is issued on `stream`
- * (a cudaStream_t, NULL for the default stream) and the call returns when it
- * is done.  Scratch lives in fixed device arrays of the library (about 21 MiB
- * on each device that loads it, kept until exit): grids above about 8.4
- * million points (1,048,576 rows of 8 points) are rejected with AG_E_INVALID.
- * All calls share those arrays and they keep the last call's contents, so
- * calls whose GPU work overlaps race; serialise them.  The first call on a
- * device performs that device's set-up; make it before any stream capture. */
+ * as for ag_emap, 16-byte aligned), d_inv_eps (8192 FP32 values of 332/eps,
+ * 16-byte aligned, or NULL for the constant dielectric), d_out (nx*ny*nz
+ * floats, 4-byte aligned); misaligned pointers are rejected with
+ * AG_E_INVALID before any CUDA call.  Work is issued on `stream` (a
+ * cudaStream_t, NULL for the default stream) and the call is synchronous: it
+ * returns when that work is done.  Scratch lives in fixed device arrays of
+ * the library (about 21 MiB on each device that loads it, kept until exit):
+ * grids above about 8.4 million points (1,048,576 rows of 8 points) are
+ * rejected with AG_E_INVALID, also before any CUDA call.  All calls share
+ * those arrays and they keep the last call's contents, so calls whose GPU
+ * work overlaps race; serialise them.  The first call on a device (and the
+ * first after its context is re-created) performs that device's set-up; make
+ * it before any stream capture.  Like ag_emap it checks the net charge: the
+ * kernel's FP64 sum of the weights it consumed must equal the input's, else
+ * AG_E_DEVICE. */
 int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps, float* d_out,
                     void* stream);
 

@@ -126,3 +126,22 @@ def test_bench_reference_arm_prints_only_on_rank0(capsys):
         steps, warmup, gpus = 1, 3, 2
     assert bench.run_reference(A(), rank=1) is None
     assert capsys.readouterr().out == ""
+
+
+def test_noalloc_rejects_misaligned_pointers_before_any_cuda_call():
+    # ag_emap_noalloc reads atoms by 16-byte bulk copies and the dielectric
+    # table as float4; a misaligned pointer is refused by the argument checks,
+    # which run before the first CUDA call (so this runs without a GPU, and
+    # the fake addresses are never dereferenced).
+    import ctypes as C
+    g = fg.Grid(9, 9, 9, 0.375)
+    L = fg.lib()
+    rc = L.ag_emap_noalloc(C.byref(g), 10, C.c_void_p(0x10008), C.c_void_p(0x20000), C.c_void_p(0x30000), None)
+    assert rc == -1 and b"16-byte aligned" in L.ag_last_error()
+    rc = L.ag_emap_noalloc(C.byref(g), 10, C.c_void_p(0x10000), C.c_void_p(0x20004), C.c_void_p(0x30000), None)
+    assert rc == -1 and b"16-byte aligned" in L.ag_last_error()
+    rc = L.ag_emap_noalloc(C.byref(g), 10, C.c_void_p(0x10000), C.c_void_p(0x20000), C.c_void_p(0x30002), None)
+    assert rc == -1 and b"4-byte aligned" in L.ag_last_error()
+    big = fg.Grid(1025, 1025, 1025, 0.375)
+    rc = L.ag_emap_noalloc(C.byref(big), 10, C.c_void_p(0x10000), None, C.c_void_p(0x30000), None)
+    assert rc == -1 and b"too large" in L.ag_last_error()
