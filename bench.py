@@ -22,11 +22,22 @@ At N=1 the line also carries two supplementary measurements:
     replayed from one CUDA graph, autotuned e-map tiles);
   "config0": the small configuration (2,000 atoms, 61^3, 6 maps), with FastGrid's
     CPU build (all host threads) and AutoGrid 4.2.1 (one thread) timed on the same
-    job in the cpu_baseline object.
+    job in the cpu_baseline object, and the engine's fastgrid4 command line timed
+    against AutoGrid 4.2.1's whole program on the same GPF;
+  "e2e_cli": the engine's fastgrid4 command line on the large configuration's
+    GPF (parse, tables, bond vectors, GPU map set, ASCII .map writing), wall
+    time and per-phase times, next to FastGrid's CPU build on the same GPF;
+  "cpu_baseline": FastGrid's CPU build on the whole large configuration (its
+    own phase times and wall time), and, as the checker, the per-map error of
+    the GPU maps against the FP64 oracle on sampled points.
 
 --impl reference times FastGrid's own CPU path (oracle/_ref/fastgrid4, built
-from the reference sources, all host threads) on a bounded sample of the same
-workload (a 161 x 161 x 21 slab of the grid) and reports the same metric.
+from the reference sources, all host threads) on the same workload and reports
+the same metric: each step is one y-slab of the 161^3 grid (odd heights, all
+161 z-planes and all 20,000 atoms), and the K timed steps together cover every
+point of the grid once, so the timed work is the whole map set.  Its inputs are written by
+oracle/synth.py, a pure-Python copy of the engine's generator (byte-identical
+files), so the reference process never loads the engine's library.
 Under torchrun (N > 1) every rank computes its own map set on its own GPU
 (replicas; weak scaling); there is no inter-GPU exchange in this path.
 """
@@ -48,18 +59,21 @@ METRIC = "map-set sec & point-atom evals/s, direct vs surrogate at stated error"
 UNIT = "point-atom evals/s"
 WORKLOAD = dict(n_atoms=20000, semi_axes=(45, 35, 30), npts=160, seed=2,
                 ligand_types="A C HD N NA OA SA S F Cl")
-SLAB_Z = 20          # CPU sample: npts 160 160 20 (161 x 161 x 21 points)
 REF_BIN = os.path.join(HERE, "oracle", "_ref", "fastgrid4")
 AG421_BIN = os.path.join(HERE, "oracle", "_ref", "autogrid4")
 C0 = dict(n_atoms=2000, semi_axes=(20, 20, 20), npts=60, seed=1)  # 61^3, ligands A C HD N OA SA
 SURR_SEEDS = list(range(900001, 900021))   # held out: training uses seeds 1000003 * s + i
 # DRAM bytes of one emap_kernel launch on this workload (ncu dram__bytes_read.sum +
-# dram__bytes_write.sum): profiles/emap_kernel_20k_161.md.
+# dram__bytes_write.sum of one captured launch).
 EMAP_TRAFFIC_BYTES = 3.13e6
+CHECK_POINTS = 3000  # sampled grid points of the per-map error against the FP64 oracle
 
 
 def surrogate_section(fg, torch, ctx, stream, flush, np):
-    """Direct vs surrogate e-map on the held-out receptors (device time, error)."""
+    """Direct vs surrogate e-map on the held-out receptors (device time, error).
+
+    Returns the section and, per receptor, (atoms, sampled point indices,
+    surrogate values, direct values) for the FP64-oracle check."""
     import ctypes as C
     g = fg.Grid(161, 161, 161, 0.375)
     npts = g.nx * g.ny * g.nz
@@ -70,6 +84,8 @@ def surrogate_section(fg, torch, ctx, stream, flush, np):
     buf = np.empty(2 * npts, dtype=np.float32)
     d_ms, s_ms, e2e_ms = [], [], []
     max_err, sq, boxes, fallback, probe_max = 0.0, 0.0, 0, 0, 0.0
+    samples = []
+    rng = np.random.default_rng(11)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     for i, seed in enumerate(SURR_SEEDS):
         x = fg.surrogate_receptor(seed, 20000)
@@ -98,6 +114,8 @@ def surrogate_section(fg, torch, ctx, stream, flush, np):
         d_ms.append(ev[0].elapsed_time(ev[1]))
         s_ms.append(ev[2].elapsed_time(ev[3]))
         err = np.abs(buf[:npts].astype(np.float64) - direct)
+        idx = np.unique(np.concatenate([rng.choice(npts, 200, replace=False), np.argsort(np.abs(direct))[-50:]]))
+        samples.append((x, idx, buf[idx].astype(np.float64), direct[idx]))
         max_err = max(max_err, float(err.max()))
         sq += float((err * err).sum())
         boxes += st["boxes"]
@@ -119,7 +137,7 @@ def surrogate_section(fg, torch, ctx, stream, flush, np):
             "probe_max_err": probe_max, "e2e_ms_host_buffers": sum(e2e_ms) / len(e2e_ms),
             "method": "exact near field within 10 A + 1.5 A far-field grid, trilinear + 3-layer 32-channel "
                       "BF16 3D-conv corrector (shipped weights), residual probes with direct-sum fallback",
-            "l2": "flushed before each timed map"}
+            "l2": "flushed before each timed map"}, samples
 
 
 def config0_section(fg, torch, ctx, stream, tmp, steps):
@@ -158,11 +176,12 @@ def config0_section(fg, torch, ctx, stream, tmp, steps):
 
 
 def config0_cpu(d):
-    """FastGrid's CPU build (all host threads) and AutoGrid 4.2.1 (one thread) on the small configuration."""
+    """FastGrid's CPU build (all host threads) and AutoGrid 4.2.1 (one thread) on the small configuration,
+    and the engine's fastgrid4 command line on the same GPF (whole programs, wall time)."""
     out = {}
     if os.path.exists(REF_BIN):
         t0 = time.perf_counter()
-        secs, _ = fastgrid_cpu_run(d, os.path.join(d, "c0.gpf"))
+        secs, _, _ = fastgrid_cpu_run(d, os.path.join(d, "c0.gpf"))
         out.update(fastgrid_cpu_map_set_s=secs, fastgrid_cpu_wall_s=time.perf_counter() - t0,
                    fastgrid_cpu_threads=os.cpu_count())
     if os.path.exists(AG421_BIN):
@@ -170,7 +189,27 @@ def config0_cpu(d):
         r = subprocess.run([AG421_BIN, "-p", "c0.gpf", "-l", "ag421.glg"], cwd=d, capture_output=True, text=True)
         if r.returncode == 0:
             out.update(autogrid421_wall_s=time.perf_counter() - t0, autogrid421_threads=1)
+    cli = cli_run(d, "c0.gpf")
+    out["engine_cli_wall_s"] = cli["wall_s"]
+    if "autogrid421_wall_s" in out:
+        out["cli_speedup_vs_autogrid421_wall"] = out["autogrid421_wall_s"] / cli["wall_s"]
+    if "fastgrid_cpu_wall_s" in out:
+        out["cli_speedup_vs_fastgrid_cpu_wall"] = out["fastgrid_cpu_wall_s"] / cli["wall_s"]
     return out
+
+
+def cli_run(workdir, gpf):
+    """The engine's fastgrid4 command line on `gpf` (a whole program: parse, tables, bond vectors, GPU
+    map set, .map/.fld/.xyz writing): wall time and its --benchmark phase times."""
+    import fastgrid_b200 as fg
+    t0 = time.perf_counter()
+    r = subprocess.run([fg.CLI_PATH, "-p", gpf, "-l", "cli.glg", "--benchmark"], cwd=workdir, capture_output=True,
+                       text=True)
+    wall = time.perf_counter() - t0
+    if r.returncode != 0:
+        raise RuntimeError("fastgrid4 (engine) failed: " + r.stderr[-500:])
+    phases = {m.group(1).strip(): float(m.group(2)) for m in re.finditer(r"^(.+?)\s+Real: ([0-9.]+) ms", r.stderr, re.M)}
+    return {"wall_s": wall, "phases_ms": phases}
 
 
 def batch_section(fg, ctx, tmp, steps, np):
@@ -226,14 +265,47 @@ def config_dict(n_gpus, extra=None):
     return d
 
 
-def make_workload(d, npts_z=None):
+def make_workload(d):
     import fastgrid_b200 as fg
-    gpf = fg.synth_write(d, "bench", **WORKLOAD)
-    if npts_z is not None:
-        txt = open(gpf).read()
-        txt = re.sub(r"^npts .*$", f"npts 160 160 {npts_z}", txt, flags=re.M)
-        open(gpf, "w").write(txt)
-    return gpf
+    return fg.synth_write(d, "bench", **WORKLOAD)
+
+
+def slab_plan(steps, planes=161):
+    """Heights of `steps` consecutive y-slabs of the grid that together cover its `planes` rows once:
+    odd heights (a GPF's npts must be even), as equal as possible; when the parities do not add up
+    the last slab reaches one plane past the top (its points are counted like the others)."""
+    steps = max(1, steps)
+    if steps >= planes:
+        return [1] * steps
+    base = planes // steps
+    if base % 2 == 0:
+        base -= 1
+    h = [base] * steps
+    k = 0
+    while sum(h) < planes:
+        h[k % steps] += 2
+        k += 1
+    return h
+
+
+def slab_gpf(src, dst, y0, height, center):
+    """Copy of the GPF `src` for rows y0 .. y0+height-1 of the 161^3 grid centred at `center` (all 161
+    z-planes, so FastGrid's OpenMP loops, which run over z, keep every host thread busy)."""
+    h = 0.375
+    cy = center[1] + (y0 + (height - 1) / 2.0 - 80) * h
+    txt = open(src).read()
+    txt = re.sub(r"^npts .*$", f"npts 160 {height - 1} 160", txt, flags=re.M)
+    txt = re.sub(r"^gridcenter .*$", f"gridcenter {center[0]:.6f} {cy:.6f} {center[2]:.6f}", txt, flags=re.M)
+    open(dst, "w").write(txt)
+
+
+def pdbqt_centroid(path):
+    xyz = []
+    for line in open(path):
+        if line.startswith(("ATOM", "HETATM")):
+            xyz.append((float(line[30:38]), float(line[38:46]), float(line[46:54])))
+    n = len(xyz)
+    return [sum(a[k] for a in xyz) / n for k in range(3)]
 
 
 class ClockSampler:
@@ -287,58 +359,112 @@ def max_over_ranks(value, dist, device):
     return float(t.item())
 
 
+FG_PHASES = ("Cutoff grid", "KD-tree of hydrogens", "Atom & desolvation maps", "Electrostatic map")
+
+
 def fastgrid_cpu_run(workdir, gpf):
-    """Run FastGrid's CPU build on `gpf`; return (map-set seconds, stderr)."""
+    """Run FastGrid's CPU build on `gpf`; return (map-set seconds, all its --benchmark phases in ms, wall s).
+    The map-set time is the sum of its e-map, cutoff-grid, kd-tree and affinity phases."""
+    t0 = time.perf_counter()
     r = subprocess.run([REF_BIN, "-p", os.path.basename(gpf), "-l", "ref.glg", "--benchmark"], cwd=workdir,
                        capture_output=True, text=True)
+    wall = time.perf_counter() - t0
     if r.returncode != 0:
         raise RuntimeError("fastgrid4 (reference CPU) failed: " + r.stderr[-500:])
-    ms = 0.0
-    for phase in ("Cutoff grid", "KD-tree of hydrogens", "Atom & desolvation maps", "Electrostatic map"):
-        m = re.search(re.escape(phase) + r"\s+Real:\s+(\d+) ms", r.stderr)
-        if m:
-            ms += float(m.group(1))
-    return ms / 1e3, r.stderr
+    phases = {m.group(1).strip(): float(m.group(2)) for m in re.finditer(r"^(.+?)\s+Real: (\d+) ms", r.stderr, re.M)}
+    return sum(phases.get(k, 0.0) for k in FG_PHASES) / 1e3, phases, wall
 
 
-def cpu_sample(tmp):
-    """FastGrid CPU on the 161 x 161 x 21 slab: (pairs/s, seconds, pairs)."""
-    d = os.path.join(tmp, "cpu_sample")
-    os.makedirs(d, exist_ok=True)
-    gpf = make_workload(d, npts_z=SLAB_Z)
-    secs, _ = fastgrid_cpu_run(d, gpf)
-    pairs = WORKLOAD["n_atoms"] * 161 * 161 * (SLAB_Z + 1)
-    return pairs / secs, secs, pairs
+def cpu_baseline_leg(tmp, gpf_dir, prob, maps, surr_samples, np):
+    """FastGrid's CPU build on the whole large configuration, and the checker: the per-map error of the
+    GPU maps against the FP64 oracle on sampled points (and of the surrogate e-maps, if measured)."""
+    import oracle
+    secs, phases, wall = fastgrid_cpu_run(gpf_dir, os.path.join(gpf_dir, "bench.gpf"))
+    pairs = WORKLOAD["n_atoms"] * 161 ** 3
+    cpu = {"value": pairs / secs, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+           "sample": f"FastGrid CPU (oracle/_ref/fastgrid4, OpenMP, all host threads) on the whole workload, "
+                     f"{pairs:.3g} pairs in {secs:.2f} s of its e-map + cutoff-grid + kd-tree + affinity phases",
+           "map_set_s": secs, "wall_s": wall, "phases_ms": phases}
+    # Checker: GPU maps against the FP64 oracle on sampled points.
+    rng = np.random.default_rng(7)
+    npts = prob.npoints
+    nm = prob.n_maps
+    e_gpu = maps[nm]
+    idx = np.unique(np.concatenate([rng.choice(npts, CHECK_POINTS, replace=False),
+                                    np.argsort(np.abs(e_gpu))[-200:]]))
+    e_ref = oracle.emap_points(prob.grid, prob.xyzw(), prob.inv_eps(), idx)
+    a_ref, d_ref = oracle.affinity_points(prob.grid, prob.receptor, prob.params, idx)
+    names = WORKLOAD["ligand_types"].split() + ["e", "d"]
+    per_map = {}
+    for m in range(nm + 2):
+        ref = a_ref[m] if m < nm else (e_ref if m == nm else d_ref)
+        d = maps[m][idx].astype(np.float64) - ref
+        per_map[names[m]] = {"max_abs": float(np.abs(d).max()), "rms": float(np.sqrt((d * d).mean())),
+                             "max_rel": float((np.abs(d) / np.maximum(np.abs(ref), 1e-3)).max())}
+    check = {"points": int(idx.size), "per_map": per_map,
+             "tolerance": "e-map 1e-4 kcal/mol/e; affinity and d-map max(1e-3, 1e-4 |v|) kcal/mol"}
+    if surr_samples:
+        smax, ssq, dmax, n = 0.0, 0.0, 0.0, 0
+        eps = oracle_ddd(np)
+        g = prob.grid.__class__(161, 161, 161, 0.375)
+        for x, sidx, sval, dval in surr_samples:
+            ref = oracle.emap_points(g, x, eps, sidx)
+            smax = max(smax, float(np.abs(sval - ref).max()))
+            ssq += float(((sval - ref) ** 2).sum())
+            dmax = max(dmax, float(np.abs(dval - ref).max()))
+            n += sidx.size
+        check["surrogate_vs_fp64_oracle"] = {"points": n, "max_abs": smax, "rms": (ssq / n) ** 0.5,
+                                             "direct_max_abs": dmax}
+    return cpu, check
+
+
+def oracle_ddd(np):
+    """332/eps table of the distance-dependent dielectric, as the oracle computes it."""
+    import oracle
+    import ctypes as C
+    t = np.empty(8192)
+    oracle.lib().oracle_ddd_table(t.ctypes.data_as(C.POINTER(C.c_double)))
+    return t
 
 
 def run_reference(args, rank):
+    """FastGrid's CPU build on the whole large configuration, one y-slab per step (rank 0 only)."""
     if rank != 0:
         return
     if not os.path.exists(REF_BIN):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fastgrid4 was not built "
                           "(build() compiles it from the reference sources when they are present)"}))
         return
+    from oracle import synth  # writes the inputs without loading the engine's library
+    heights = slab_plan(args.steps)
     with tempfile.TemporaryDirectory() as tmp:
-        d = os.path.join(tmp, "ref")
-        os.makedirs(d)
-        gpf = make_workload(d, npts_z=SLAB_Z)
-        pairs = WORKLOAD["n_atoms"] * 161 * 161 * (SLAB_Z + 1)
-        for _ in range(args.warmup):
-            fastgrid_cpu_run(d, gpf)
-        times = [fastgrid_cpu_run(d, gpf)[0] for _ in range(args.steps)]
-    secs = sum(times) / len(times)
+        src = synth.write(tmp, "bench", **WORKLOAD)
+        center = pdbqt_centroid(os.path.join(tmp, "bench.pdbqt"))
+        gpf = os.path.join(tmp, "slab.gpf")
+        for _ in range(args.warmup):  # one row of x-z points through the middle
+            slab_gpf(src, gpf, 80, 1, center)
+            fastgrid_cpu_run(tmp, gpf)
+        times, y0 = [], 0
+        for hgt in heights:
+            slab_gpf(src, gpf, y0 % 161, hgt, center)
+            times.append(fastgrid_cpu_run(tmp, gpf)[0])
+            y0 += hgt
+    planes = sum(heights)
+    pairs = WORKLOAD["n_atoms"] * 161 * 161 * planes
+    secs = sum(times)
     value = pairs / secs
     cores = os.cpu_count()
-    sample = (f"161x161x21 z-slab of the 161^3 grid (all 20000 atoms, {pairs:.3g} point-atom pairs) per step; "
-              "map-set time = FastGrid's own e-map + cutoff-grid + kd-tree + affinity phase times")
+    sample = (f"the whole 161^3 grid in {len(heights)} y-slabs of {min(heights)}-{max(heights)} rows, one per "
+              f"step ({planes} rows, all 20000 atoms each step, {pairs:.3g} point-atom pairs); time = FastGrid's "
+              "own e-map + cutoff-grid + kd-tree + affinity phase times; inputs written by oracle/synth.py")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_dict(args.gpus, {"sample": sample}),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_dict(args.gpus),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "map_set_sec_sample": secs}))
+        "map_set_sec_whole_grid": secs}))
 
 
 def main():
@@ -437,37 +563,55 @@ def main():
             t0 = time.perf_counter()
             prob.compute(ctx)
             e2e_t.append(time.perf_counter() - t0)
-        outp = prob.maps().reshape(-1)
+        maps_all = prob.maps().reshape(nmaps + 2, npts)
         e2e_s = max_over_ranks(sum(e2e_t) / len(e2e_t), dist, f"cuda:{local}")
         e2e_value = world * pairs / e2e_s
-        check = float(np.abs(outp[nmaps * npts:(nmaps + 1) * npts]).max())
-
-        # ---- CPU baseline (rank 0, N=1 only) ----
-        cpu = None
-        if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
-            v, secs, sp = cpu_sample(tmp)
-            cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": f"FastGrid CPU (oracle/_ref/fastgrid4, OpenMP) on the 161x161x21 z-slab, {sp:.3g} "
-                             f"pairs in {secs:.2f} s of e-map + affinity phases"}
-
+        check = float(np.abs(maps_all[nmaps]).max())
         emap_pairs_per_s = pairs / (emap_avg * 1e-3)
         ck = clocks.summary()
 
         # ---- supplementary measurements (N=1) ----
         surr = batch = None
+        surr_samples = []
         if world == 1 and not args.no_surrogate:
-            surr = surrogate_section(fg, torch, ctx, stream, flush, np)
+            surr, surr_samples = surrogate_section(fg, torch, ctx, stream, flush, np)
         if world == 1 and not args.no_batch:
             batch = batch_section(fg, ctx, tmp, args.steps, np)
         c0 = c0dir = None
         if world == 1 and not args.no_config0:
             c0, c0dir = config0_section(fg, torch, ctx, stream, tmp, args.steps)
-        if cpu is not None and c0dir is not None:
-            cpu["config0"] = config0_cpu(c0dir)
-            if c0 is not None and "fastgrid_cpu_map_set_s" in cpu["config0"]:
-                c0["speedup_vs_fastgrid_cpu"] = cpu["config0"]["fastgrid_cpu_map_set_s"] / (c0["map_set_ms"] * 1e-3)
-            if c0 is not None and "autogrid421_wall_s" in cpu["config0"]:
-                c0["speedup_vs_autogrid421"] = cpu["config0"]["autogrid421_wall_s"] / (c0["e2e_ms"] * 1e-3)
+
+        # ---- CPU baseline and checker (rank 0, N=1 only), then the command line end to end ----
+        cpu = check_maps = e2e_cli = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_BIN):
+            cpu, check_maps = cpu_baseline_leg(tmp, tmp, prob, maps_all, surr_samples, np)
+            for f in os.listdir(tmp):
+                if f.endswith(".map"):
+                    os.remove(os.path.join(tmp, f))
+            if c0dir is not None:
+                cpu["config0"] = config0_cpu(c0dir)
+                if c0 is not None and "fastgrid_cpu_map_set_s" in cpu["config0"]:
+                    c0["speedup_vs_fastgrid_cpu_map_set"] = (cpu["config0"]["fastgrid_cpu_map_set_s"] /
+                                                             (c0["map_set_ms"] * 1e-3))
+            if surr is not None and "surrogate_vs_fp64_oracle" in check_maps:
+                surr["vs_fp64_oracle"] = check_maps.pop("surrogate_vs_fp64_oracle")
+        if rank == 0 and world == 1:
+            d = os.path.join(tmp, "cli")
+            os.makedirs(d, exist_ok=True)
+            for f in ("bench.gpf", "bench.pdbqt"):
+                shutil.copy(os.path.join(tmp, f), os.path.join(d, f))
+            e2e_cli = cli_run(d, "bench.gpf")
+            e2e_cli["workload"] = "the large configuration's GPF through the engine's fastgrid4 command line"
+            e2e_cli["value"] = pairs / e2e_cli["wall_s"]
+            e2e_cli["unit"] = UNIT
+            host = {k: v for k, v in e2e_cli["phases_ms"].items() if k not in ("Total", "Grid maps (GPU)")}
+            if host:
+                e2e_cli["largest_host_phase"] = max(host, key=host.get)
+            if cpu is not None:
+                e2e_cli["fastgrid_cpu_wall_s"] = cpu["wall_s"]
+                e2e_cli["speedup_vs_fastgrid_cpu_wall"] = cpu["wall_s"] / e2e_cli["wall_s"]
+            shutil.rmtree(d, ignore_errors=True)
+
         if rank == 0:
             line = {
                 "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -478,7 +622,7 @@ def main():
                 "roofline": {"bound": "sfu", "kernel": "emap_kernel",
                              "achieved": emap_pairs_per_s / 1e9, "peak": rsqrt_ps / 1e9, "unit": "Gpair/s",
                              "frac": emap_pairs_per_s / rsqrt_ps, "traffic": EMAP_TRAFFIC_BYTES,
-                             "traffic_unit": "bytes per launch (ncu, profiles/emap_kernel_20k_161.md)",
+                             "traffic_unit": "DRAM bytes per launch (ncu capture of this workload)",
                              "note": "one SFU rsqrt per point-atom pair; peak = rsqrt/s measured by "
                                      "ag_measure_peaks in this run (MEASURED_PEAKS.json has no SFU figure)"},
                 "roofline_fp32": {"achieved_ops": 8 * emap_pairs_per_s / 1e12, "peak": ffma_ps / 1e12,
@@ -486,7 +630,8 @@ def main():
                                   "note": "8 algorithmic FP32-pipe ops per pair vs measured FFMA issue rate"},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_s * 1e3},
-                "gpu_launches": launches, "clocks": ck, "cpu_baseline": cpu,
+                "gpu_launches": launches, "clocks": ck, "cpu_baseline": cpu, "e2e_cli": e2e_cli,
+                "check_vs_fp64_oracle": check_maps,
                 "emap_abs_max": check, "surrogate": surr, "batch": batch, "config0": c0,
             }
             print(json.dumps(line))

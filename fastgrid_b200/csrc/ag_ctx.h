@@ -104,6 +104,8 @@ struct ag_ctx {
   int ctasPerSm = agk::kEmapCtasPerSm;
   agc::DevBuf<double> checksum;
   int checksumSplits = 0;
+  int testIdleWait = 0;             // test hook AG_TUNE_TEST_IDLE_WAIT
+  double testChecksumOffset = 0;    // test hook AG_TUNE_TEST_CHECKSUM_OFFSET
   double wSum = 0, wAbsSum = 0, lastChecksum = 0;
   agc::SurrState* surr = nullptr;
   cudaStream_t copyStream = nullptr;  // device-to-host copies that overlap compute (whole-job path)

@@ -65,6 +65,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
   return false;
 }
 
+// The same with an explicit poll limit (a test hook uses a few polls on a
+// barrier nothing arrives on, to make the expiry path run).
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t* bar, unsigned parity, unsigned* status, int limit) {
+  for (int i = 0; i < limit; i++)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(status, ST_WAIT_TIMEOUT);
+  return false;
+}
+
 __device__ __forceinline__ float rsqrt_approx(float x) {
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));

@@ -144,7 +144,8 @@ struct Problem {
 // operations.  Writes the .xyz file on the `gridcenter` line like the reference.
 void loadGPF(Problem& p, ParamLib& lib, Log& log, const char* gpfPath);
 // Tables, desolvation function, bond vectors (main.cpp:163-193 order).
-void precompute(Problem& p, ParamLib& lib, Log& log);
+// phaseMs (optional): [0] pair-energy and desolvation tables, [1] bond vectors, in ms.
+void precompute(Problem& p, ParamLib& lib, Log& log, double* phaseMs = nullptr);
 
 // Output
 void writeFld(const Problem& p, const char* programName, Log& log);

@@ -40,6 +40,7 @@ struct EmapParams {
   float2 negBias2;                // -2^23, both halves: bin = f + negBias2
   float2 negLambda2;              // -0.3153767175 / 100 / ln 2, both halves: E = 2^(negLambda2 * bin)
   float2 poly2[6];                // invEps(bin) = sum_n poly2[n] E^n (both halves equal) for E <= 0.031
+  int testIdleWait;               // test hook: > 0 adds a wait of that many polls on a barrier nothing arrives on
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1
   unsigned* status;

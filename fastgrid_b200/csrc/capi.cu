@@ -190,6 +190,14 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "tcgen05 switch must be 0 or 1");
       agc::surrUseTc(c, v != 0.0);
       return AG_OK;
+    case AG_TUNE_TEST_IDLE_WAIT:
+      if (!(v >= 0.0 && v <= 64.0) || v != (double)(int)v) return fail(AG_E_INVALID, "idle-wait polls must be 0..64");
+      c->testIdleWait = (int)v;
+      return AG_OK;
+    case AG_TUNE_TEST_CHECKSUM_OFFSET:
+      if (!std::isfinite(v)) return fail(AG_E_INVALID, "checksum offset must be finite");
+      c->testChecksumOffset = v;
+      return AG_OK;
     case AG_TUNE_EMAP_CTAS_PER_SM:
       if (!(v >= 1.0 && v <= 8.0)) return fail(AG_E_INVALID, "CTAs per SM must be 1..8");
       c->ctasPerSm = (int)v;
@@ -389,6 +397,7 @@ int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P)
   }
   P.out = dOut;
   P.status = c->status.p;
+  P.testIdleWait = c->testIdleWait;
   // Split atoms across CTAs when the grid alone cannot fill the GPU.
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -673,8 +682,9 @@ int checkStatus(ag_ctx* c) {
     for (double v : cs) s += v;
     c->checksumSplits = 0;
     c->lastChecksum = s;
-    if (!(std::fabs(s - c->wSum) <= 1e-9 * c->wAbsSum + 1e-12))
-      return fail(AG_E_DEVICE, "net-charge checksum mismatch: kernel summed %.17g, input holds %.17g", s, c->wSum);
+    const double want = c->wSum + c->testChecksumOffset;
+    if (!(std::fabs(s - want) <= 1e-9 * c->wAbsSum + 1e-12))
+      return fail(AG_E_DEVICE, "net-charge checksum mismatch: kernel summed %.17g, input holds %.17g", s, want);
   }
   return AG_OK;
 }
@@ -910,6 +920,8 @@ struct ag_batch {
   DevBuf<agk::AffParams> ajobs;
   DevBuf<int2> aunits;
   DevBuf<int> counters;
+  DevBuf<double> checks;                 // per job: net-charge checksum of its e-map (FP64 weight sum)
+  std::vector<double> hChecks;
   int ne = 0, na = 0, nmPadMax = 4, nmapsMax = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -945,12 +957,13 @@ int batchBuild(ag_batch* b) {
   b->nmPadMax = 4;
   b->nmapsMax = 0;
   b->pairs = 0;
+  CK(b->checks.ensure(b->sub.size()));
   for (size_t i = 0; i < b->sub.size(); i++) {
     ag_ctx* c = b->sub[i];
     const int64_t np = c->npoints();
     agk::EmapParams P;
     if (int e = buildEmapParams(c, c->maps.p + (size_t)c->nMaps * np, false, P)) return e;
-    P.checksum = nullptr;
+    P.checksum = b->checks.p + i;  // written by the job's first CTA box (no atom split in a batch)
     const int j = (int)ej.size();
     ej.push_back(P);
     for (int k = 0; k < P.nblocks; k++)
@@ -1039,6 +1052,9 @@ extern "C" int ag_batch_compute(ag_batch* b) {
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ctx->device);
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int err = AG_OK;
+    // NaN in every checksum slot until the job's e-map writes it.
+    if (cudaMemsetAsync(b->checks.p, 0xFF, sizeof(double) * b->sub.size(), st) != cudaSuccess)
+      err = fail(AG_E_CUDA, "batch checksum reset failed");
     for (ag_ctx* c : b->sub)
       if (!err) err = prepAffinity(c, st);
     if (!err && agk::emap_batch_launch(b->ejobs.p, b->eunits.p, b->ne, b->counters.p, 2 * sms, st) != cudaSuccess)
@@ -1073,6 +1089,16 @@ extern "C" int ag_batch_compute(ag_batch* b) {
   for (ag_ctx* c : b->sub) {
     c->checksumSplits = 0;
     if (int e = checkStatus(c)) return e;
+  }
+  // Net-charge checksum of every job's e-map: the FP64 sum of the weights its
+  // kernel consumed must equal the host's sum of the job's input weights.
+  b->hChecks.resize(b->sub.size());
+  CK(cudaMemcpy(b->hChecks.data(), b->checks.p, sizeof(double) * b->sub.size(), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < b->sub.size(); i++) {
+    const ag_ctx* c = b->sub[i];
+    if (!(std::fabs(b->hChecks[i] - c->wSum) <= 1e-9 * c->wAbsSum + 1e-12))
+      return fail(AG_E_DEVICE, "net-charge checksum mismatch in batch job %d: kernel summed %.17g, input holds %.17g",
+                  (int)i, b->hChecks[i], c->wSum);
   }
   return AG_OK;
 }
@@ -1165,6 +1191,7 @@ extern "C" int ag_batch_free(ag_batch* b) {
   b->ajobs.release();
   b->aunits.release();
   b->counters.release();
+  b->checks.release();
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   for (ag_ctx* c : b->sub) ag_ctx_destroy(c);
@@ -1283,12 +1310,23 @@ int runMain(int argc, char** argv) {
   ag::ParamLib lib(v4);
   Timer t0;
   ag::loadGPF(p, lib, log, gpf.empty() ? nullptr : gpf.c_str());
-  ag::precompute(p, lib, log);
+  const double parseMs = t0.ms();
+  double preMs[2] = {0, 0};
+  ag::precompute(p, lib, log, preMs);
+  Timer tf;
   ag::writeFld(p, prog, log);
-  if (bench) fprintf(stderr, "Precalculations          Real: %.0f ms\n", t0.ms());
+  const double fldMs = tf.ms();
+  if (bench) {
+    fprintf(stderr, "Parsing GPF and PDBQT    Real: %.1f ms\n", parseMs);
+    fprintf(stderr, "Energy tables            Real: %.1f ms\n", preMs[0]);
+    fprintf(stderr, "Bond vectors             Real: %.1f ms\n", preMs[1]);
+    fprintf(stderr, "Writing .fld             Real: %.1f ms\n", fldMs);
+  }
 
+  Timer tc;
   ag_ctx* ctx = nullptr;
   if (ag_ctx_create(dev, &ctx) != AG_OK) log.fatal(-2, "%s", ag_last_error());
+  if (bench) fprintf(stderr, "CUDA context             Real: %.1f ms\n", tc.ms());
   ag_problem P;
   P.p = std::move(p);
   for (auto& m : P.p.maps) {
@@ -1307,14 +1345,14 @@ int runMain(int argc, char** argv) {
   const double gpuMs = t1.ms();
   ag_ctx_destroy(ctx);
   if (bench) {
-    fprintf(stderr, "Grid maps (GPU)          Real: %.0f ms\n", gpuMs);
+    fprintf(stderr, "Grid maps (GPU)          Real: %.1f ms\n", gpuMs);
     double pairs = (double)P.p.numAtoms * (double)P.p.numPoints;
     fprintf(stderr, "Electrostatics performance: %i million atoms/s (whole map set)\n", (int)(pairs / (gpuMs * 1e-3) / 1e6));
   }
   Timer t2;
   for (int m = 0; m < P.p.numMaps() + 2; m++) ag::writeMap(P.p, m, log);
   ag::writeFloatingGrid(P.p, log);
-  if (bench) fprintf(stderr, "Saving maps              Real: %.0f ms\n", t2.ms());
+  if (bench) fprintf(stderr, "Saving maps              Real: %.1f ms\n", t2.ms());
 
   // Summary of extrema (GridMap.cpp:53-82), over the rounded values.
   log.print("\nGrid\tAtom\tMinimum   \tMaximum\nMap \tType\tEnergy    \tEnergy \n\t\t(kcal/mol)\t(kcal/mol)\n____\t____\t_____________\t_____________\n");
@@ -1332,7 +1370,7 @@ int runMain(int argc, char** argv) {
   log.print("\n\n * Note:  Every pairwise-atomic interaction was clamped at %.2f\n\n\n", ag::kEintClamp);
   fprintf(stderr, "\n%s: Successful Completion.\n", prog);
   log.print("%s: Successful Completion.\n", prog);
-  if (bench) fprintf(stderr, "Total                    Real: %.0f ms\n", total.ms());
+  if (bench) fprintf(stderr, "Total                    Real: %.1f ms\n", total.ms());
   return 0;
 }
 

@@ -55,6 +55,7 @@ struct EmapSmem {
   double wpart[kThreads / 32];
   int unit;                       // persistent batch kernel: the unit being processed
   uint64_t bar[2];
+  uint64_t barIdle;               // never arrived on (target of the expiry test hook)
 };
 
 __device__ __forceinline__ void unpack_item(int v, int& xc, int& y, int& z) {
@@ -228,6 +229,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
   if (tid == 0) {
     mbar_init(&S.bar[0], 1);
     mbar_init(&S.bar[1], 1);
+    mbar_init(&S.barIdle, 1);
     fence_barrier_init();
   }
   __syncthreads();
@@ -259,6 +261,9 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       tma_load_1d(S.ring[slot ^ 1], P.atoms + t1, n1 * 32u, &S.bar[slot ^ 1]);
     }
     bool ok = mbar_wait_bounded(&S.bar[slot], (unsigned)(t >> 1) & 1u, P.status);
+    // Test hook: after the first tile has landed, wait a few polls on a
+    // barrier that nothing arrives on; the wait expires like a lost copy would.
+    if (P.testIdleWait > 0 && t == 0) ok = mbar_wait_limit(&S.barIdle, 0u, P.status, P.testIdleWait) && ok;
     if (__syncthreads_or(!ok)) {
       // Give the copies still in flight (this tile's and the prefetched next
       // one) a bounded chance to land before shared memory is released.

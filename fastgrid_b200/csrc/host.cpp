@@ -5,6 +5,7 @@
 #include "ag_host.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cctype>
 #include <cmath>
 #include <cstdarg>
@@ -715,7 +716,7 @@ void bondVectors(Problem& p, const ParamLib& lib, Log& log) {
 
 }  // namespace
 
-void precompute(Problem& p, ParamLib& lib, Log& log) {
+void precompute(Problem& p, ParamLib& lib, Log& log, double* phaseMs) {
   // A GPF "parameter_file" is read only now, after the GPF (main.cpp:170-171):
   // it can change coeff_desolv and it resets the receptor indices that the bond
   // vectors and the disordered-hydrogen test look up by type name.
@@ -727,11 +728,18 @@ void precompute(Problem& p, ParamLib& lib, Log& log) {
       throw;
     }
   }
+  const auto t0 = std::chrono::steady_clock::now();
   energyTables(p);
   desolvTable(p, lib.coeff_desolv);
+  const auto t1 = std::chrono::steady_clock::now();
   bondVectors(p, lib, log);
+  const auto t2 = std::chrono::steady_clock::now();
   p.hydrogen = lib.recIndexOf("HD");
   if (!p.distDepDiel && p.epsilon.empty()) p.epsilon.assign(kMaxDist, 0.0);
+  if (phaseMs) {
+    phaseMs[0] = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    phaseMs[1] = std::chrono::duration<double, std::milli>(t2 - t1).count();
+  }
 }
 
 // ---------------------------------------------------------------------------

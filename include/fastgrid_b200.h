@@ -97,6 +97,15 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
                                          neighbouring lanes sharing a 16-point x span alternately (default 2) */
 #define AG_TUNE_EMAP_TILE 5           /* direct e-map: TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 20816) */
 #define AG_TUNE_SURROGATE_TCGEN05 6   /* 0/1: surrogate corrector convolutions on tcgen05 (1, default) or mma.sync (0) */
+/* Failure-detection test hooks (default 0 = off).  IDLE_WAIT: 1..64 polls of an
+ * extra wait, after each direct e-map CTA's first atom tile has landed, on a
+ * barrier nothing arrives on; the wait expires, the kernel records it in its
+ * status word, lets its own copies land and returns, and the call fails with
+ * AG_E_DEVICE.  CHECKSUM_OFFSET: added to the host's FP64 sum of the input
+ * weights before the net-charge checksum comparison, so a nonzero value makes
+ * the call fail with AG_E_DEVICE. */
+#define AG_TUNE_TEST_IDLE_WAIT 7
+#define AG_TUNE_TEST_CHECKSUM_OFFSET 8
 int ag_ctx_tune(ag_ctx* ctx, int knob, double value);
 
 /* ------------------------------------------------------------------------ */

@@ -92,5 +92,8 @@ def round3(a):
 def read_map(path):
     """Values of an AutoGrid .map file (6 header lines, one value per line)."""
     with open(path, "rb") as f:
-        lines = f.read().replace(b"\r", b"").split(b"\n")
-    return np.array([float(x) for x in lines[6:] if x.strip()])
+        b = f.read().replace(b"\r", b"")
+    pos = 0
+    for _ in range(6):
+        pos = b.index(b"\n", pos) + 1
+    return np.fromstring(b[pos:].decode(), dtype=np.float64, sep="\n")

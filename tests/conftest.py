@@ -18,8 +18,8 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = os.path.join(REPO, "tests", "golden")
 sys.path.insert(0, REPO)
 
-CASES = ["colagen2", "hsg1_sm", "synth_c0", "synth_const_diel", "synth_covalent", "synth_paramfile_v4",
-         "synth_disorder_h"]
+CASES = ["colagen2", "hsg1_sm", "1pgp", "x1hpv", "synth_c0", "synth_const_diel", "synth_covalent",
+         "synth_paramfile_v4", "synth_disorder_h"]
 
 # Tolerances (unrounded values against the FP64 oracle):
 #   electrostatics: 1e-4 kcal/mol/e absolute
@@ -64,6 +64,19 @@ def materialize(name, dest):
         with open(os.path.join(dest, "hsg1_sm.gpf"), "w") as f:
             f.write(case["gpf"])
         return dest, "hsg1_sm.gpf", case
+    if "files_dir" in case:  # reference test receptors: files (some xz-compressed) + the GPF
+        for f in case["files"]:
+            src = os.path.join(GOLDEN, case["files_dir"], f)
+            if f.endswith(".xz"):
+                with open(os.path.join(dest, f[:-3]), "wb") as o:
+                    o.write(lzma.decompress(open(src, "rb").read()))
+            else:
+                shutil.copy(src, os.path.join(dest, f))
+                os.chmod(os.path.join(dest, f), 0o644)
+        stem = name + ".gpf"
+        with open(os.path.join(dest, stem), "w") as f:
+            f.write(case["gpf"])
+        return dest, stem, case
     import fastgrid_b200 as fg
     gen = dict(case["gen"])
     gen["semi_axes"] = tuple(gen["semi_axes"])
@@ -105,6 +118,12 @@ def golden_values(rec):
         v = np.array(rec["values"], dtype=np.int64)
         return np.arange(v.size), v
     return np.array(rec["sample_idx"], dtype=np.int64), np.array(rec["sample_values"], dtype=np.int64)
+
+
+def golden_tol(rec):
+    """Allowed difference in thousandths between a golden map and the reference
+    restatement: 0 (exact), k, or None when the map is not pinned."""
+    return rec.get("tol", 0)
 
 
 def map_names(case):

@@ -1,7 +1,8 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference.
 
-Run in the build container (needs /root/reference and the reference programs
-built by ``make -C oracle ref``):
+Run in the build container (needs the reference checkout — $FASTGRID_REFERENCE,
+default /root/reference — and the reference programs built by
+``make -C oracle ref``):
 
     python tests/golden/make_golden.py
 
@@ -12,6 +13,17 @@ Fixtures written (all small):
   hsg1_sm.json + hsg1_sm/           AutoGrid 4.2.1's test case
       (AG421/Tests/hsg1_sm.gpf, hsg1_sm.pdbqt, AD4.1_bound.dat, golden maps
       py_hsg1_sm.*.map).
+  1pgp.json + 1pgp/                 AutoDock 4.0.1's test receptor
+      (autogrid_original_r1_tag/autodock-4.0.1/Tests/1pgp.gpf, 1pgp_rec.pdbqt,
+      AD4_parameters.dat, golden maps 1pgp_rec.{C,HD,OA,P,e,d}.map, run with
+      --v4).  Written by AutoGrid 4.0, so only the e-map and d-map are pinned
+      exactly; C and P agree within 8 thousandths (AutoGrid 4.0 rounding of the
+      pair-energy tables) and HD and OA follow AutoGrid 4.0's older H-bond
+      model, so they are not pinned ("tol": null).
+  x1hpv.json + x1hpv/               AutoGrid 4.2.1's GPF tests x1hpv_CASE0..3
+      (AG421/Tests/test_autogrid4.py:281-311): CASE0 must complete (golden maps
+      = FastGrid's CPU build on it), CASE1-3 lack a map / elecmap / dsolvmap
+      line and must fail.
   synth_*.json                      seeded synthetic receptors (regenerated by the
       tests from their parameters) with the maps FastGrid's CPU build
       (oracle/_ref/fastgrid4) writes for them.
@@ -35,16 +47,18 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
-REF = "/root/reference"
+REF = os.environ.get("FASTGRID_REFERENCE", "/root/reference")
 FG4 = os.path.join(REPO, "oracle", "_ref", "fastgrid4")
 
 import fastgrid_b200 as fg  # noqa: E402  (generator only)
 from oracle import read_map  # noqa: E402
 
 
-def map_record(values, full_limit=1000, nsample=600, seed=0):
+def map_record(values, full_limit=1000, nsample=600, seed=0, tol=0):
+    """tol: 0 = pinned exactly (hash and values); k > 0 = pinned within k thousandths;
+    None = not pinned (stored for reference only)."""
     k = np.round(np.asarray(values) * 1000.0).astype(np.int64)
-    rec = {"n": int(k.size), "sha256": hashlib.sha256(k.tobytes()).hexdigest()}
+    rec = {"n": int(k.size), "sha256": hashlib.sha256(k.tobytes()).hexdigest(), "tol": tol}
     if k.size <= full_limit:
         rec["values"] = k.tolist()
     else:
@@ -90,6 +104,47 @@ def hsg1_sm():
     for m in maps + [e, d]:
         out["maps"][m] = map_record(read_map(os.path.join(t, "py_" + m)))
     json.dump(out, open(os.path.join(HERE, "hsg1_sm.json"), "w"))
+
+
+def pgp1():
+    t = os.path.join(REF, "autogrid_original_r1_tag", "autodock-4.0.1", "Tests")
+    dst = os.path.join(HERE, "1pgp")
+    os.makedirs(dst, exist_ok=True)
+    with open(os.path.join(dst, "1pgp_rec.pdbqt.xz"), "wb") as f:
+        f.write(lzma.compress(open(os.path.join(t, "1pgp_rec.pdbqt"), "rb").read(), preset=9))
+    shutil.copy(os.path.join(t, "AD4_parameters.dat"), os.path.join(dst, "AD4_parameters.dat"))
+    gpf = open(os.path.join(t, "1pgp.gpf")).read()
+    maps, e, d = gpf_maps(gpf)
+    tol = {"1pgp_rec.C.map": 8, "1pgp_rec.P.map": 8, "1pgp_rec.HD.map": None, "1pgp_rec.OA.map": None}
+    out = {"gpf": gpf, "v4": True, "files_dir": "1pgp", "files": ["1pgp_rec.pdbqt.xz", "AD4_parameters.dat"],
+           "maps": {}, "source": "autogrid_original_r1_tag/autodock-4.0.1/Tests/1pgp_rec.*.map (AutoGrid 4.0 golden)"}
+    for m in maps + [e, d]:
+        out["maps"][m] = map_record(read_map(os.path.join(t, m)), tol=tol.get(m, 0))
+    json.dump(out, open(os.path.join(HERE, "1pgp.json"), "w"))
+
+
+def x1hpv():
+    t = os.path.join(REF, "autogrid_original_4_2_1_ref", "autogrid", "Tests")
+    dst = os.path.join(HERE, "x1hpv")
+    os.makedirs(dst, exist_ok=True)
+    with open(os.path.join(dst, "x1hpv.pdbqt.xz"), "wb") as f:
+        f.write(lzma.compress(open(os.path.join(t, "x1hpv.pdbqt"), "rb").read(), preset=9))
+    gpfs = {c: open(os.path.join(t, f"x1hpv_CASE{c}.gpf")).read() for c in range(4)}
+    tmp = tempfile.mkdtemp()
+    try:
+        shutil.copy(os.path.join(t, "x1hpv.pdbqt"), tmp)
+        open(os.path.join(tmp, "x1hpv.gpf"), "w").write(gpfs[0])
+        r = subprocess.run([FG4, "-p", "x1hpv.gpf", "-l", "ref.glg"], cwd=tmp, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        maps, e, d = gpf_maps(gpfs[0])
+        out = {"gpf": gpfs[0], "v4": False, "files_dir": "x1hpv", "files": ["x1hpv.pdbqt.xz"], "maps": {},
+               "negative": {f"x1hpv_CASE{c}.gpf": gpfs[c] for c in (1, 2, 3)},
+               "source": "AG421/Tests/x1hpv_CASE0.gpf run by oracle/_ref/fastgrid4 (FastGrid CPU build)"}
+        for m in maps + [e, d]:
+            out["maps"][m] = map_record(read_map(os.path.join(tmp, m)))
+        json.dump(out, open(os.path.join(HERE, "x1hpv.json"), "w"))
+    finally:
+        shutil.rmtree(tmp)
 
 
 # Synthetic cases: generator parameters + GPF edits; golden = FastGrid CPU.
@@ -168,6 +223,8 @@ def synth(name, spec):
 if __name__ == "__main__":
     colagen2()
     hsg1_sm()
+    pgp1()
+    x1hpv()
     for n, s in SYNTH.items():
         synth(n, s)
     print("fixtures written to", HERE)

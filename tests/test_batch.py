@@ -1,9 +1,12 @@
 """GPU: batches of map sets (persistent kernels under one CUDA graph).
 
 Six receptors of uneven atom counts and grid sizes are computed as one batch;
-every map set must match the single-job path (same tolerances as the parity
-tests), a replay of the captured graph must reproduce the first run bit for
-bit, and the autotuner's cache file must round-trip.
+every map set must match the FP64 oracle (every point of the grids up to
+51^3, 2,000 sampled points of the larger ones; the parity tests' tolerances)
+and the single-job path, a replay of the captured graph must reproduce the
+first run bit for bit, and the autotuner's cache file must round-trip.  Every
+batch computation also passes the net-charge checksum of each job's e-map
+(ag_batch_compute fails otherwise).
 """
 import os
 
@@ -13,6 +16,7 @@ import pytest
 from conftest import AFF_ABS, AFF_REL, E_TOL, chdir
 
 import fastgrid_b200 as fg
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +33,25 @@ def _problems(tmp):
     return out
 
 
-def test_batch_matches_single_jobs(tmp_path):
+def _check_against_oracle(p, got, i):
+    nm = p.n_maps
+    if p.grid.nx <= 51:
+        idx = np.arange(p.npoints)
+        om, od = oracle.affinity(p.grid, p.receptor, p.params)
+        oe = oracle.emap(p.grid, p.xyzw(), p.inv_eps())
+    else:
+        idx = np.sort(np.random.default_rng(i).choice(p.npoints, 2000, replace=False))
+        om, od = oracle.affinity_points(p.grid, p.receptor, p.params, idx)
+        oe = oracle.emap_points(p.grid, p.xyzw(), p.inv_eps(), idx)
+    flat = got.reshape(nm + 2, -1)
+    for m in range(nm):
+        d = np.abs(flat[m, idx] - om[m])
+        assert (d <= np.maximum(AFF_ABS, AFF_REL * np.abs(om[m]))).all(), (i, m, d.max())
+    assert np.abs(flat[nm, idx] - oe).max() <= E_TOL, (i, np.abs(flat[nm, idx] - oe).max())
+    assert (np.abs(flat[nm + 1, idx] - od) <= np.maximum(AFF_ABS, AFF_REL * np.abs(od))).all(), i
+
+
+def test_batch_matches_oracle_and_single_jobs(tmp_path):
     ctx = fg.Context(0)
     probs = _problems(tmp_path)
     single = []
@@ -45,6 +67,7 @@ def test_batch_matches_single_jobs(tmp_path):
         assert np.array_equal(again, first[i]), f"graph replay differs for job {i}"
         ref = single[i].astype(np.float64)
         got = first[i].astype(np.float64)
+        _check_against_oracle(p, got, i)
         nm = p.n_maps
         d = np.abs(got[:nm] - ref[:nm])
         assert (d <= np.maximum(AFF_ABS, AFF_REL * np.abs(ref[:nm]))).all(), (i, d.max())

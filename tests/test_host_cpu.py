@@ -145,3 +145,66 @@ def test_noalloc_rejects_misaligned_pointers_before_any_cuda_call():
     big = fg.Grid(1025, 1025, 1025, 0.375)
     rc = L.ag_emap_noalloc(C.byref(big), 10, C.c_void_p(0x10000), None, C.c_void_p(0x30000), None)
     assert rc == -1 and b"too large" in L.ag_last_error()
+
+
+@pytest.mark.parametrize("seed,kw", [
+    (1, dict(n_atoms=2000, semi_axes=(20, 20, 20), npts=60)),
+    (2, dict(n_atoms=20000, semi_axes=(45, 35, 30), npts=160, ligand_types="A C HD N NA OA SA S F Cl")),
+    (7000, dict(n_atoms=1800, semi_axes=(17, 17, 17), npts=44, ligand_types="A C HD N OA SA")),
+])
+def test_python_generator_writes_the_same_files(tmp_path, seed, kw):
+    """oracle/synth.py (used by bench.py's reference arm, which must not load
+    the engine's library) writes byte-identical PDBQT and GPF files."""
+    from oracle import synth
+    fg.synth_write(str(tmp_path / "lib"), "s", seed=seed, **kw)
+    synth.write(str(tmp_path / "py"), "s", seed=seed, **kw)
+    for ext in (".pdbqt", ".gpf"):
+        assert open(tmp_path / "lib" / ("s" + ext), "rb").read() == open(tmp_path / "py" / ("s" + ext), "rb").read()
+
+
+def test_reference_arm_slabs_cover_the_grid_once():
+    sys.path.insert(0, REPO)
+    import bench
+    for k in (1, 2, 3, 5, 20, 25, 161):
+        h = bench.slab_plan(k)
+        assert len(h) == k and all(x % 2 == 1 for x in h)
+        assert 161 <= sum(h) <= 162
+    assert "fastgrid_b200" not in open(os.path.join(REPO, "oracle", "synth.py")).read().split('"""')[2]
+
+
+@pytest.mark.parametrize("gpf,message", [("x1hpv_CASE1.gpf", "Not enough map keywords found"),
+                                         ("x1hpv_CASE2.gpf", "No electrostatic map file defined"),
+                                         ("x1hpv_CASE3.gpf", "No desolvation map file defined")])
+def test_cli_rejects_gpf_missing_a_map_line(tmp_path, gpf, message):
+    """AutoGrid 4.2.1's negative GPF tests (Tests/test_autogrid4.py:299-311):
+    a GPF with one map / elecmap / dsolvmap line missing must not complete.
+    The loader stops before any GPU work, like FastGrid's CPU build (exit
+    code -2, as the shell sees it 254)."""
+    from conftest import materialize
+    work, _, case = materialize("x1hpv", str(tmp_path))
+    open(os.path.join(work, gpf), "w").write(case["negative"][gpf])
+    r = subprocess.run([fg.CLI_PATH, "-p", gpf, "-l", "neg.glg"], cwd=work, capture_output=True, text=True)
+    assert r.returncode == 254, r.stderr
+    assert message in r.stderr
+    assert "Successful Completion" not in open(os.path.join(work, "neg.glg")).read()
+
+
+def test_cli_timeout_ends_a_stalled_job(tmp_path):
+    """--timeout N (ProgramParameters.cpp:199-220): the job runs in a child
+    process; if it has not finished after N seconds the parent kills it,
+    prints "Timeout! Process terminated." and exits 0.  The job stalls on the
+    host: its receptor file is a FIFO that nobody writes, so it never reaches
+    the GPU."""
+    fifo = tmp_path / "stall.pdbqt"
+    os.mkfifo(fifo)
+    (tmp_path / "stall.gpf").write_text("npts 4 4 4\ngridfld stall.maps.fld\nspacing 0.375\n"
+                                        "receptor_types A C\nligand_types C\nreceptor stall.pdbqt\n"
+                                        "gridcenter 0 0 0\nmap stall.C.map\nelecmap stall.e.map\n"
+                                        "dsolvmap stall.d.map\ndielectric -0.1465\n")
+    t0 = __import__("time").perf_counter()
+    r = subprocess.run([fg.CLI_PATH, "--timeout", "1", "-p", "stall.gpf", "-l", "stall.glg"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=60)
+    dt = __import__("time").perf_counter() - t0
+    assert r.returncode == 0
+    assert "Timeout! Process terminated." in r.stderr
+    assert 0.9 <= dt < 20
