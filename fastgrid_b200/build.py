@@ -17,7 +17,7 @@ OUT = os.path.join(HERE, "_lib")
 OBJ = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU = ["emap.cu", "affinity.cu", "cells.cu", "capi.cu", "peaks.cu", "emap_noalloc.cu", "surrogate.cu",
+CU = ["emap.cu", "affinity.cu", "affinity2.cu", "cells.cu", "capi.cu", "peaks.cu", "emap_noalloc.cu", "surrogate.cu",
       "surrogate_host.cu", "surr_near.cu", "surr_tc.cu"]
 CPP = ["host.cpp", "synth.cpp"]
 LIB = os.path.join(OUT, "libfastgrid_b200.so")

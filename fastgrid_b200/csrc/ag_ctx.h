@@ -77,6 +77,8 @@ struct ag_ctx {
   uint64_t atomsVersion = 0;      // bumped whenever new atoms are staged
   // affinity
   agc::DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
+  agc::DevBuf<int> ctStart, ctAtoms;  // type-major cell list ((cell, type) segments) of the two-point kernel
+  int affKernel = 2;                  // affinity kernel: 2 two-point (default), 1 one point per thread
   agc::DevBuf<float> vol, solq, affTab, affTabH, sol, rv32, rv2_32;
   agc::DevBuf<double> rv64, thrA;
   struct Pass {

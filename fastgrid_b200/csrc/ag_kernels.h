@@ -136,8 +136,61 @@ struct CellBuild {
   int* cellAtoms;                 // n_atoms
   int* fill;                      // ncell scratch
   const int* donorMask;           // optional: only atoms with mask[i] != 0 (null = all)
+  const int* typeInfo;            // optional: key = cell * ntypes + (typeInfo[i] & 31) (type-major segments)
+  int ntypes;
 };
+// ncellTotal: number of keys (cells, or cells x ntypes with typeInfo).
 cudaError_t cells_launch(const CellBuild& C, int ncellTotal, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Affinity + desolvation, two grid points per thread (affinity2.cu)
+// ---------------------------------------------------------------------------
+constexpr int kA2Slots = 4;         // H-bond maps per pass handled by the two-point kernel
+enum { A2_SPH = 0, A2_D1 = 1, A2_A1 = 2, A2_A2 = 3 };          // angular class of a receptor type
+enum { A2_SLOT_ACC = 0, A2_SLOT_A1 = 1, A2_SLOT_DON = 2 };     // H-bond map kind (probe class)
+
+struct Aff2Params {
+  // receptor (device)
+  const double4* xyz;             // FP64 grid-centred x, y, z
+  const int* info;                // type | hbond << 5 | disorder << 8 | rexp << 9
+  const float* vol;
+  const float* solq;
+  const float* rv;                // rvector (FP32, 3 per atom)
+  const float* rv2;               // rvector2 (FP32, 3 per atom)
+  const double* rv64;             // rvector (FP64) for exact sign decisions
+  // type-major cell list: segment (cell, type) = atoms ctAtoms[ctStart[cell*ntypes+t] .. ctStart[...+1])
+  const int* ctStart;
+  const int* ctAtoms;
+  double cellLo[3];
+  int ncell[3];
+  // grid
+  int nx, ny, nz, n2x, n2y, n2z;
+  int64_t npoints;
+  double h;
+  // maps of this pass
+  int nmaps, nmPad, ntypes, hydrogen;
+  const float* table;             // [ntypes][kAffRows][nmPad] FP32
+  const float* tableH;            // [kAffRows][nmPad] rows of the "HD" type, or null
+  const float* sol;               // kAffRows
+  const double* thr;              // affinity bin thresholds (kAffRows + 1)
+  float delta;                    // guard half-width around bin edges (bins)
+  int needClosestH;               // some D1 type meets an acceptor-probe slot: find the nearest donor
+  int typeAng[kMaxTypes];         // A2_SPH / A2_D1 / A2_A1 / A2_A2
+  int typeDonor[kMaxTypes];       // DS or D1 (candidates of the nearest-donor search)
+  unsigned typeSlots[kMaxTypes];  // bit k: H-bond slot k applies to this type
+  unsigned typePlain[kMaxTypes];  // bit g: map g takes the plain table sum for this type
+  int nslots;
+  int slotMap[kA2Slots];          // map index of each H-bond slot
+  int slotKind[kA2Slots];         // A2_SLOT_*
+  int mapCov[kMaxMapsPass];
+  float solparProbe[kMaxMapsPass], volProbe[kMaxMapsPass];
+  float solparQ;
+  float* out;                     // this pass's first map: [nmaps][npoints]
+  float* dmap;
+  unsigned* status;
+};
+size_t aff2_smem_bytes(int nmPad);
+cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st);
 
 struct ClosestHParams {
   const double4* xyz;

@@ -153,7 +153,7 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   c->blocks.release();
   c->status.release();
   for (auto* b : {&c->items, &c->info, &c->cellStart, &c->cellAtoms, &c->cellOf, &c->count, &c->fill, &c->dStart,
-                  &c->dAtoms, &c->donorMask, &c->closestH})
+                  &c->dAtoms, &c->donorMask, &c->closestH, &c->ctStart, &c->ctAtoms})
     b->release();
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->copyStream) cudaStreamDestroy(c->copyStream);
@@ -189,6 +189,10 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
     case AG_TUNE_SURROGATE_TCGEN05:
       if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "tcgen05 switch must be 0 or 1");
       agc::surrUseTc(c, v != 0.0);
+      return AG_OK;
+    case AG_TUNE_AFFINITY_KERNEL:
+      if (!(v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "affinity kernel must be 1 or 2");
+      c->affKernel = (int)v;
       return AG_OK;
     case AG_TUNE_TEST_IDLE_WAIT:
       if (!(v >= 0.0 && v <= 64.0) || v != (double)(int)v) return fail(AG_E_INVALID, "idle-wait polls must be 0..64");
@@ -566,7 +570,42 @@ void cellGrid(const ag_grid& g, double lo[3], int ncell[3]) {
   }
 }
 
-// Cell lists (all atoms, H donors) and the nearest donor of every point, on stream st.
+// H-bond slots of a pass for the two-point kernel: the H-bond maps whose term
+// differs from a plain table sum for some receptor type
+// (CalculateGridmaps.cpp:206-228).  Returns false if the pass has more than
+// kA2Slots of them (the one-point kernel then computes it).
+bool passSlots(const ag_ctx* c, const ag_ctx::Pass& ps, int& nslots, int slotMap[agk::kA2Slots],
+               int slotKind[agk::kA2Slots]) {
+  nslots = 0;
+  for (int g = 0; g < ps.nm; g++) {
+    const int m = ps.m0 + g, mhb = c->mapHbond[m];
+    if (!c->mapIsHB[m] || c->mapCov[m]) continue;
+    int kind = -1;
+    if (mhb == ag::AS || mhb == ag::A2) kind = agk::A2_SLOT_ACC;
+    else if (mhb == ag::A1) kind = agk::A2_SLOT_A1;
+    else if (mhb == ag::DS || mhb == ag::D1) kind = agk::A2_SLOT_DON;
+    if (kind < 0) continue;
+    if (nslots == agk::kA2Slots) return false;
+    slotMap[nslots] = g;
+    slotKind[nslots] = kind;
+    nslots++;
+  }
+  return true;
+}
+
+// Whether every affinity pass of the staged job runs on the two-point kernel.
+bool useTwoPoint(const ag_ctx* c) {
+  if (c->affKernel != 2) return false;
+  for (const auto& ps : c->passes) {
+    int n, sm[agk::kA2Slots], sk[agk::kA2Slots];
+    if (!passSlots(c, ps, n, sm, sk)) return false;
+  }
+  return true;
+}
+
+// Cell lists on stream st.  One-point kernel: all atoms and H donors in 8 A
+// cells, and the nearest donor of every point.  Two-point kernel: one list of
+// (cell, receptor type) segments (it finds the nearest donor itself).
 int prepAffinity(ag_ctx* c, cudaStream_t st) {
   const ag_grid& g = c->grid;
   const int64_t np = c->npoints();
@@ -576,13 +615,24 @@ int prepAffinity(ag_ctx* c, cudaStream_t st) {
   int ncell[3];
   cellGrid(g, lo, ncell);
   const int ncellT = ncell[0] * ncell[1] * ncell[2];
+  agk::CellBuild C{};
+  C.xyz = c->atoms.p; C.n_atoms = n;
+  for (int d = 0; d < 3; d++) { C.lo[d] = lo[d]; C.ncell[d] = ncell[d]; }
+  if (useTwoPoint(c)) {
+    const int nkeys = ncellT * c->nTypes;
+    CK(c->ctStart.ensure(nkeys + 1)); CK(c->count.ensure(nkeys + 1)); CK(c->fill.ensure(nkeys + 1));
+    CK(c->ctAtoms.ensure(n)); CK(c->cellOf.ensure(n));
+    C.cellOf = c->cellOf.p; C.count = c->count.p; C.fill = c->fill.p;
+    C.cellStart = c->ctStart.p; C.cellAtoms = c->ctAtoms.p; C.donorMask = nullptr;
+    C.typeInfo = c->info.p; C.ntypes = c->nTypes;
+    CK(agk::cells_launch(C, nkeys, st));
+    c->launches += 4;
+    return AG_OK;
+  }
   CK(c->cellStart.ensure(ncellT + 1)); CK(c->count.ensure(ncellT + 1)); CK(c->fill.ensure(ncellT + 1));
   CK(c->cellAtoms.ensure(n)); CK(c->cellOf.ensure(n));
   CK(c->dStart.ensure(ncellT + 1)); CK(c->dAtoms.ensure(n));
   CK(c->closestH.ensure(np));
-  agk::CellBuild C{};
-  C.xyz = c->atoms.p; C.n_atoms = n;
-  for (int d = 0; d < 3; d++) { C.lo[d] = lo[d]; C.ncell[d] = ncell[d]; }
   C.cellOf = c->cellOf.p; C.count = c->count.p; C.fill = c->fill.p;
   C.cellStart = c->cellStart.p; C.cellAtoms = c->cellAtoms.p; C.donorMask = nullptr;
   CK(agk::cells_launch(C, ncellT, st));
@@ -596,6 +646,70 @@ int prepAffinity(ag_ctx* c, cudaStream_t st) {
   H.npoints = np; H.h = h; H.closestH = c->closestH.p;
   CK(agk::closest_h_launch(H, st));
   c->launches += 1;
+  return AG_OK;
+}
+
+// Launch parameters of the two-point kernel for the staged job's passes.
+int buildAff2Params(ag_ctx* c, float* dMaps, float* dDmap, std::vector<agk::Aff2Params>& out) {
+  const ag_grid& g = c->grid;
+  double lo[3];
+  int ncell[3];
+  cellGrid(g, lo, ncell);
+  out.clear();
+  const int nt = c->nTypes;
+  std::vector<ag_ctx::Pass> passes = c->passes;
+  if (passes.empty()) {  // no ligand maps: one pass for the d-map alone
+    ag_ctx::Pass ps{};
+    ps.nmPad = 4;
+    passes.push_back(ps);
+  }
+  for (const auto& ps : passes) {
+    agk::Aff2Params P{};
+    P.xyz = c->atoms.p; P.info = c->info.p; P.vol = c->vol.p; P.solq = c->solq.p;
+    P.rv = c->rv32.p; P.rv2 = c->rv2_32.p; P.rv64 = c->rv64.p;
+    P.ctStart = c->ctStart.p; P.ctAtoms = c->ctAtoms.p;
+    for (int d = 0; d < 3; d++) { P.cellLo[d] = lo[d]; P.ncell[d] = ncell[d]; }
+    P.nx = g.nx; P.ny = g.ny; P.nz = g.nz; P.n2x = g.nx / 2; P.n2y = g.ny / 2; P.n2z = g.nz / 2;
+    P.npoints = c->npoints(); P.h = g.spacing;
+    P.nmaps = ps.nm; P.nmPad = ps.nmPad; P.ntypes = nt; P.hydrogen = c->hydrogen;
+    P.table = c->affTab.p + ps.tabOff;
+    P.tableH = (c->hydrogen >= 0 && c->hydrogen < nt) ? c->affTabH.p + ps.tabHOff : nullptr;
+    P.sol = c->sol.p;
+    P.thr = c->thrA.p;
+    P.delta = 1.0e-3f;
+    if (!passSlots(c, ps, P.nslots, P.slotMap, P.slotKind)) return fail(AG_E_INVALID, "too many H-bond maps");
+    for (int k = P.nslots; k < agk::kA2Slots; k++) { P.slotMap[k] = -1; P.slotKind[k] = agk::A2_SLOT_ACC; }
+    P.needClosestH = 0;
+    for (int t = 0; t < agk::kMaxTypes; t++) {
+      const int ahb = t < nt ? c->typeHbond[t] : ag::NON;
+      const bool donor = ahb == ag::DS || ahb == ag::D1, acceptor = ahb >= ag::AS;
+      unsigned slots = 0;
+      for (int k = 0; k < P.nslots; k++)
+        if (((P.slotKind[k] == agk::A2_SLOT_ACC || P.slotKind[k] == agk::A2_SLOT_A1) && donor) ||
+            (P.slotKind[k] == agk::A2_SLOT_DON && acceptor))
+          slots |= 1u << k;
+      unsigned plain = 0;
+      for (int gg = 0; gg < ps.nm; gg++) plain |= 1u << gg;
+      for (int k = 0; k < P.nslots; k++)
+        if ((slots >> k) & 1u) plain &= ~(1u << P.slotMap[k]);
+      P.typeSlots[t] = slots;
+      P.typePlain[t] = plain;
+      P.typeDonor[t] = donor ? 1 : 0;
+      P.typeAng[t] = ahb == ag::D1 ? agk::A2_D1 : ahb == ag::A1 ? agk::A2_A1 : ahb == ag::A2 ? agk::A2_A2 : agk::A2_SPH;
+      for (int k = 0; k < P.nslots; k++)
+        if (((slots >> k) & 1u) && P.slotKind[k] == agk::A2_SLOT_ACC && ahb == ag::D1) P.needClosestH = 1;
+    }
+    for (int k = 0; k < agk::kMaxMapsPass; k++) {
+      P.mapCov[k] = k < ps.nm ? c->mapCov[ps.m0 + k] : 1;
+      P.solparProbe[k] = k < ps.nm ? (float)c->solparProbe[ps.m0 + k] : 0.f;
+      P.volProbe[k] = k < ps.nm ? (float)c->volProbe[ps.m0 + k] : 0.f;
+    }
+    P.solparQ = (float)c->solparQ;
+    P.out = dMaps + (size_t)ps.m0 * c->npoints();
+    P.dmap = dDmap;
+    P.status = c->status.p;
+    out.push_back(P);
+  }
   return AG_OK;
 }
 
@@ -654,6 +768,15 @@ int buildAffParams(ag_ctx* c, float* dMaps, float* dDmap, std::vector<agk::AffPa
 
 int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
   if (int e = prepAffinity(c, c->stream)) return e;
+  if (useTwoPoint(c)) {
+    std::vector<agk::Aff2Params> passes;
+    if (int e = buildAff2Params(c, dMaps, dDmap, passes)) return e;
+    for (const auto& P : passes) {
+      CK(agk::aff2_launch(P, c->stream));
+      c->launches += 1;
+    }
+    return AG_OK;
+  }
   std::vector<agk::AffParams> passes;
   if (int e = buildAffParams(c, dMaps, dDmap, passes)) return e;
   for (const auto& P : passes) {
@@ -1024,6 +1147,7 @@ extern "C" int ag_batch_create(ag_ctx* ctx, ag_problem* const* problems, int n, 
     }
     ag_ctx* c = nullptr;
     if (int e = ag_ctx_create(ctx->device, &c)) { ag_batch_free(b); return e; }
+    c->affKernel = 1;  // the persistent batch kernel works on the one-point kernel's cell lists
     b->sub.push_back(c);
     b->probs.push_back(problems[i]);
     ag_grid g;

@@ -22,7 +22,8 @@ __device__ __forceinline__ double rsq_exact_c(double ax, double ay, double az, d
 }
 
 // ---------------------------------------------------------------------------
-// Cell list: counting sort into 8 A cells; file order inside each cell.
+// Cell list: counting sort into 8 A cells (or into (cell, type) segments);
+// file order inside each cell or segment.
 // ---------------------------------------------------------------------------
 __global__ void cell_count_kernel(CellBuild C) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < C.n_atoms; i += gridDim.x * blockDim.x) {
@@ -31,8 +32,10 @@ __global__ void cell_count_kernel(CellBuild C) {
       const double4 a = C.xyz[i];
       const int cx = (int)floor((a.x - C.lo[0]) / 8.0), cy = (int)floor((a.y - C.lo[1]) / 8.0),
                 cz = (int)floor((a.z - C.lo[2]) / 8.0);
-      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < C.ncell[0] && cy < C.ncell[1] && cz < C.ncell[2])
+      if (cx >= 0 && cy >= 0 && cz >= 0 && cx < C.ncell[0] && cy < C.ncell[1] && cz < C.ncell[2]) {
         cell = (cz * C.ncell[1] + cy) * C.ncell[0] + cx;
+        if (C.typeInfo) cell = cell * C.ntypes + (C.typeInfo[i] & 31);
+      }
     }
     C.cellOf[i] = cell;
     if (cell >= 0) atomicAdd(&C.count[cell], 1);

@@ -97,6 +97,10 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
                                          neighbouring lanes sharing a 16-point x span alternately (default 2) */
 #define AG_TUNE_EMAP_TILE 5           /* direct e-map: TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 20816) */
 #define AG_TUNE_SURROGATE_TCGEN05 6   /* 0/1: surrogate corrector convolutions on tcgen05 (1, default) or mma.sync (0) */
+#define AG_TUNE_AFFINITY_KERNEL 9     /* affinity pass: 2 two grid points per thread, type-major candidates,
+                                         nearest donor found in the kernel (default); 1 one point per thread
+                                         with a separate nearest-donor kernel (also used for passes with more
+                                         than 4 H-bond maps) */
 /* Failure-detection test hooks (default 0 = off).  IDLE_WAIT: 1..64 polls of an
  * extra wait, after each direct e-map CTA's first atom tile has landed, on a
  * barrier nothing arrives on; the wait expires, the kernel records it in its

@@ -69,6 +69,49 @@ def test_map_set_matches_oracle_and_golden(name, tmp_path, ctx):
         assert ok.all(), f"{name} {n}: written values differ at {idx[~ok][:5]}"
 
 
+@pytest.mark.parametrize("name", ["colagen2", "hsg1_sm", "synth_disorder_h", "synth_paramfile_v4"])
+def test_one_point_affinity_kernel_matches_oracle(name, tmp_path):
+    """The one-point affinity kernel (a separate nearest-donor kernel, one
+    grid point per thread), still used for passes with more than four H-bond
+    maps and by the batch kernel, against the oracle (the default two-point
+    kernel is covered by the test above)."""
+    from test_oracle import oracle_maps
+    work, gpf, case = materialize(name, str(tmp_path))
+    with chdir(work):
+        p = fg.Problem(gpf, v4=case["v4"], log="glg.txt")
+    c = fg.Context(0)
+    try:
+        c.tune(fg.AG_TUNE_AFFINITY_KERNEL, 1)
+        p.compute(c)
+    finally:
+        c.close()
+    names, en, dn = map_names(case)
+    _check_maps(p.maps().reshape(p.n_maps + 2, -1), oracle_maps(p, case), names, en, dn, name + " (one-point)")
+
+
+def test_many_hbond_maps(tmp_path):
+    """Seven H-bond probe maps (HD HS NA NS OA OS SA): more than the two-point
+    kernel's four H-bond slots, so that pass falls back to the one-point
+    kernel; both settings must match the oracle."""
+    fg.synth_write(str(tmp_path), "hb", n_atoms=1500, semi_axes=(14, 13, 12), npts=30, seed=17,
+                   ligand_types="A C HD HS NA NS OA OS SA")
+    with chdir(str(tmp_path)):
+        p = fg.Problem("hb.gpf", log="hb.glg")
+    om, od = oracle.affinity(p.grid, p.receptor, p.params)
+    for k in (2, 1):
+        c = fg.Context(0)
+        try:
+            c.tune(fg.AG_TUNE_AFFINITY_KERNEL, k)
+            p.compute(c)
+        finally:
+            c.close()
+        gpu = p.maps().reshape(p.n_maps + 2, -1).astype(np.float64)
+        for m in range(p.n_maps):
+            d = np.abs(gpu[m] - om[m])
+            assert (d <= np.maximum(AFF_ABS, AFF_REL * np.abs(om[m]))).all(), (k, m, d.max())
+        assert (np.abs(gpu[p.n_maps + 1] - od) <= np.maximum(AFF_ABS, AFF_REL * np.abs(od))).all(), k
+
+
 def test_emap_edge_cases(ctx):
     """Atoms on a grid point, within 0.01 A of one, at r = 0.5 A (the 1/r cap),
     beyond 81.91 A (the table clamp), and grids that are not multiples of the
