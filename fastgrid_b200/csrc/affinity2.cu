@@ -277,9 +277,10 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
 
 size_t aff2_smem_bytes(int nmPad) { return tabOffset() + sizeof(float) * (size_t)(kAffRows + 1) * nmPad; }
 
+// One work unit: the CTA block `cta` of job P.  Called once per CTA by
+// affinity2_kernel and repeatedly by the persistent batch kernel.
 template <int NMAX>
-__global__ void __launch_bounds__(kT, 2) affinity2_kernel(const __grid_constant__ Aff2Params P) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
+__device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, unsigned char* smem_raw) {
   A2Smem& S = *reinterpret_cast<A2Smem*>(smem_raw);
   float* tab = reinterpret_cast<float*>(smem_raw + tabOffset());
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -288,7 +289,6 @@ __global__ void __launch_bounds__(kT, 2) affinity2_kernel(const __grid_constant_
 
   // This CTA's 8 x 8 x 8 points; this warp's 4 x 4 x 4 sub-box; this thread's two points.
   const int tbx = (P.nx + 7) / 8, tby = (P.ny + 7) / 8;
-  const int cta = blockIdx.x;
   const int x0 = (cta % tbx) * 8, y0 = ((cta / tbx) % tby) * 8, z0 = (cta / (tbx * tby)) * 8;
   const int wx = x0 + (warp & 1) * 4, wy = y0 + ((warp >> 1) & 1) * 4, wz = z0 + (warp >> 2) * 4;
   Pts<NMAX> q;
@@ -594,6 +594,52 @@ __global__ void __launch_bounds__(kT, 2) affinity2_kernel(const __grid_constant_
     }
     P.dmap[pt] = P.solparQ * q.s1[p];
   }
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(kT, 2) affinity2_kernel(const __grid_constant__ Aff2Params P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  aff2_unit<NMAX>(P, blockIdx.x, smem_raw);
+}
+
+// Persistent kernel over the work units (job, CTA block) of a batch of
+// receptors, taken from an atomic counter in the host's (decreasing cost) order.
+template <int NMAX>
+__global__ void __launch_bounds__(kT, 2)
+    affinity2_batch_kernel(const Aff2Params* __restrict__ jobs, const int2* __restrict__ units, int nunits,
+                           int* counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int s_unit;
+  for (;;) {
+    __syncthreads();  // the previous unit is finished by every thread
+    if (threadIdx.x == 0) s_unit = atomicAdd(counter, 1);
+    __syncthreads();
+    const int u = s_unit;
+    if (u >= nunits) return;
+    const int2 w = units[u];
+    aff2_unit<NMAX>(jobs[w.x], w.y, smem_raw);
+  }
+}
+
+int aff2_ctas(int nx, int ny, int nz) { return ((nx + 7) / 8) * ((ny + 7) / 8) * ((nz + 7) / 8); }
+
+cudaError_t aff2_batch_launch(const Aff2Params* jobs, const int2* units, int nunits, int* counter, int nmPadMax,
+                              int nmapsMax, int grid, cudaStream_t st) {
+  const size_t smem = aff2_smem_bytes(nmPadMax);
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), st);
+  if (e != cudaSuccess) return e;
+#define AG_AFF2B(N)                                                                                               \
+  do {                                                                                                            \
+    e = cudaFuncSetAttribute(affinity2_batch_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (e != cudaSuccess) return e;                                                                               \
+    affinity2_batch_kernel<N><<<grid, kT, smem, st>>>(jobs, units, nunits, counter);                              \
+  } while (0)
+  if (nmapsMax <= 4) AG_AFF2B(4);
+  else if (nmapsMax <= 8) AG_AFF2B(8);
+  else if (nmapsMax <= 12) AG_AFF2B(12);
+  else AG_AFF2B(16);
+#undef AG_AFF2B
+  return cudaGetLastError();
 }
 
 cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st) {

@@ -191,6 +191,11 @@ struct Aff2Params {
 };
 size_t aff2_smem_bytes(int nmPad);
 cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st);
+// CTA blocks (work units) of the two-point kernel on an nx x ny x nz grid.
+int aff2_ctas(int nx, int ny, int nz);
+// Persistent two-point pass over the units (job, CTA block) of many jobs.
+cudaError_t aff2_batch_launch(const Aff2Params* jobs, const int2* units, int nunits, int* counter, int nmPadMax,
+                              int nmapsMax, int grid, cudaStream_t st);
 
 struct ClosestHParams {
   const double4* xyz;

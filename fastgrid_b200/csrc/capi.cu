@@ -1041,6 +1041,8 @@ struct ag_batch {
   DevBuf<agk::EmapParams> ejobs;
   DevBuf<int2> eunits;
   DevBuf<agk::AffParams> ajobs;
+  DevBuf<agk::Aff2Params> a2jobs;        // two-point affinity jobs (when every job allows it)
+  bool twoPoint = false;
   DevBuf<int2> aunits;
   DevBuf<int> counters;
   DevBuf<double> checks;                 // per job: net-charge checksum of its e-map (FP64 weight sum)
@@ -1076,6 +1078,7 @@ int batchBuild(ag_batch* b) {
   batchDropGraph(b);
   std::vector<agk::EmapParams> ej;
   std::vector<agk::AffParams> aj;
+  std::vector<agk::Aff2Params> a2j;
   std::vector<std::pair<double, int2>> eu, au;
   b->nmPadMax = 4;
   b->nmapsMax = 0;
@@ -1092,6 +1095,19 @@ int batchBuild(ag_batch* b) {
     for (int k = 0; k < P.nblocks; k++)
       eu.push_back({(double)c->nAtoms * c->hBlocks[k].nitems, make_int2(j, k)});
     b->pairs += (double)c->nAtoms * (double)np;
+    if (b->twoPoint) {
+      std::vector<agk::Aff2Params> passes;
+      if (int e = buildAff2Params(c, c->maps.p, c->maps.p + (size_t)(c->nMaps + 1) * np, passes)) return e;
+      const int ncta = agk::aff2_ctas(c->grid.nx, c->grid.ny, c->grid.nz);
+      for (const auto& A : passes) {
+        const int ja = (int)a2j.size();
+        a2j.push_back(A);
+        b->nmPadMax = std::max(b->nmPadMax, A.nmPad);
+        b->nmapsMax = std::max(b->nmapsMax, A.nmaps);
+        for (int k = 0; k < ncta; k++) au.push_back({(double)c->nAtoms, make_int2(ja, k)});
+      }
+      continue;
+    }
     std::vector<agk::AffParams> passes;
     if (int e = buildAffParams(c, c->maps.p, c->maps.p + (size_t)(c->nMaps + 1) * np, passes)) return e;
     const int ncta = ((c->grid.nx + agk::kAffTX - 1) / agk::kAffTX) * ((c->grid.ny + agk::kAffTY - 1) / agk::kAffTY) *
@@ -1116,12 +1132,15 @@ int batchBuild(ag_batch* b) {
   b->ne = (int)eul.size();
   b->na = (int)aul.size();
   CK(b->ejobs.ensure(ej.size()));
-  CK(b->ajobs.ensure(aj.size()));
+  CK(b->ajobs.ensure(std::max<size_t>(aj.size(), 1)));
+  CK(b->a2jobs.ensure(std::max<size_t>(a2j.size(), 1)));
   CK(b->eunits.ensure(eul.size()));
   CK(b->aunits.ensure(aul.size()));
   CK(b->counters.ensure(2));
   CK(cudaMemcpy(b->ejobs.p, ej.data(), sizeof(agk::EmapParams) * ej.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(b->ajobs.p, aj.data(), sizeof(agk::AffParams) * aj.size(), cudaMemcpyHostToDevice));
+  if (!aj.empty()) CK(cudaMemcpy(b->ajobs.p, aj.data(), sizeof(agk::AffParams) * aj.size(), cudaMemcpyHostToDevice));
+  if (!a2j.empty())
+    CK(cudaMemcpy(b->a2jobs.p, a2j.data(), sizeof(agk::Aff2Params) * a2j.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b->eunits.p, eul.data(), sizeof(int2) * eul.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(b->aunits.p, aul.data(), sizeof(int2) * aul.size(), cudaMemcpyHostToDevice));
   return AG_OK;
@@ -1147,7 +1166,7 @@ extern "C" int ag_batch_create(ag_ctx* ctx, ag_problem* const* problems, int n, 
     }
     ag_ctx* c = nullptr;
     if (int e = ag_ctx_create(ctx->device, &c)) { ag_batch_free(b); return e; }
-    c->affKernel = 1;  // the persistent batch kernel works on the one-point kernel's cell lists
+    c->affKernel = ctx->affKernel;
     b->sub.push_back(c);
     b->probs.push_back(problems[i]);
     ag_grid g;
@@ -1156,6 +1175,13 @@ extern "C" int ag_batch_create(ag_ctx* ctx, ag_problem* const* problems, int n, 
     const double* eps = nullptr;
     ag_problem_views(problems[i], &g, &r, &a, &eps);
     if (int e = ag_upload(c, &g, &r, &a, eps)) { ag_batch_free(b); return e; }
+  }
+  // One affinity kernel for the whole batch: the two-point one if every job's
+  // passes allow it.
+  b->twoPoint = true;
+  for (ag_ctx* c : b->sub) b->twoPoint = b->twoPoint && useTwoPoint(c);
+  for (ag_ctx* c : b->sub) {
+    if (!b->twoPoint) c->affKernel = 1;
     // Allocate every per-job buffer now (the graph capture must not allocate).
     if (int e = prepAffinity(c, c->stream)) { ag_batch_free(b); return e; }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) { ag_batch_free(b); return fail(AG_E_CUDA, "staging failed"); }
@@ -1183,9 +1209,14 @@ extern "C" int ag_batch_compute(ag_batch* b) {
       if (!err) err = prepAffinity(c, st);
     if (!err && agk::emap_batch_launch(b->ejobs.p, b->eunits.p, b->ne, b->counters.p, 2 * sms, st) != cudaSuccess)
       err = fail(AG_E_CUDA, "batch e-map launch failed");
-    if (!err && agk::aff_batch_launch(b->ajobs.p, b->aunits.p, b->na, b->counters.p + 1, b->nmPadMax, b->nmapsMax,
-                                      2 * sms, st) != cudaSuccess)
-      err = fail(AG_E_CUDA, "batch affinity launch failed");
+    if (!err) {
+      const cudaError_t ae =
+          b->twoPoint ? agk::aff2_batch_launch(b->a2jobs.p, b->aunits.p, b->na, b->counters.p + 1, b->nmPadMax,
+                                               b->nmapsMax, 2 * sms, st)
+                      : agk::aff_batch_launch(b->ajobs.p, b->aunits.p, b->na, b->counters.p + 1, b->nmPadMax,
+                                              b->nmapsMax, 2 * sms, st);
+      if (ae != cudaSuccess) err = fail(AG_E_CUDA, "batch affinity launch failed");
+    }
     cudaGraph_t g = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (err) {
@@ -1316,6 +1347,7 @@ extern "C" int ag_batch_free(ag_batch* b) {
   b->aunits.release();
   b->counters.release();
   b->checks.release();
+  b->a2jobs.release();
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   for (ag_ctx* c : b->sub) ag_ctx_destroy(c);
