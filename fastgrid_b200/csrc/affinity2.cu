@@ -59,6 +59,8 @@ struct A2Smem {
   int cellBeg[kCellGroup];
   int cnt[kW];
   float sol[kAffRows + 1];           // + 0 at kAffRows (the out-of-cutoff entry)
+  float4 mask4[kMaxMapsPass / 4];    // current type: 1 for maps summed plainly, 0 for its H-bond slot maps
+  float4 rch[kT][2];                 // per thread and point: rvector of the nearest H donor
   uint64_t bar;
 };
 
@@ -87,8 +89,7 @@ struct Pts {
   float px, py, pz[2];
   int ix, iy, iz0;
   bool valid[2];
-  int ch[2];                         // nearest H donor, or -1
-  float rc[2][3];                    // its rvector
+  int ch[2];                         // nearest H donor, or -1 (its rvector is in shared memory)
   float2 em[2][NMAX / 2];            // plain map sums, maps (2i, 2i+1)
   float s1[2], s2[2];                // desolvation sums (sol * vol, sol * solq)
   float mn[2][kA2Slots], mx[2][kA2Slots];  // per slot: additive sum (acceptor probes) or min / max
@@ -103,12 +104,8 @@ __device__ __forceinline__ double gcoord(int i, int n2, double h) { return __dmu
 template <int NMAX, int ANG, bool ISH>
 __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, const float* tab, const int j0,
                                          const int j1, const unsigned short* wl, const unsigned slots,
-                                         const unsigned plain, Pts<NMAX>& q) {
+                                         Pts<NMAX>& q) {
   const int nmPad = P.nmPad;
-  float2 mask[NMAX / 2];
-#pragma unroll
-  for (int g = 0; g < NMAX / 2; g++)
-    mask[g] = make_float2((plain >> (2 * g)) & 1u ? 1.f : 0.f, (plain >> (2 * g + 1)) & 1u ? 1.f : 0.f);
   const float4* tab4 = reinterpret_cast<const float4*>(tab);
   const int rowQ = nmPad >> 2;       // float4 per row
 
@@ -167,13 +164,16 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
       const float sv = S.sol[iR[p]];
       q.s1[p] = fmaf(sv, v.x, q.s1[p]);
       q.s2[p] = fmaf(sv, v.y, q.s2[p]);
-      const float4* row = tab4 + iR[p] * rowQ;
+    }
 #pragma unroll
-      for (int g4 = 0; g4 < NMAX / 4; g4++) {
-        if (4 * g4 >= P.nmaps) break;
-        const float4 e4 = row[g4];
-        q.em[p][2 * g4] = __ffma2_rn(make_float2(e4.x, e4.y), mask[2 * g4], q.em[p][2 * g4]);
-        q.em[p][2 * g4 + 1] = __ffma2_rn(make_float2(e4.z, e4.w), mask[2 * g4 + 1], q.em[p][2 * g4 + 1]);
+    for (int g4 = 0; g4 < NMAX / 4; g4++) {
+      if (4 * g4 >= P.nmaps) break;
+      const float4 m4 = S.mask4[g4];  // same address in every lane: one broadcast for both points
+#pragma unroll
+      for (int p = 0; p < 2; p++) {
+        const float4 e4 = tab4[iR[p] * rowQ + g4];
+        q.em[p][2 * g4] = __ffma2_rn(make_float2(e4.x, e4.y), make_float2(m4.x, m4.y), q.em[p][2 * g4]);
+        q.em[p][2 * g4 + 1] = __ffma2_rn(make_float2(e4.z, e4.w), make_float2(m4.z, m4.w), q.em[p][2 * g4 + 1]);
       }
     }
     if (slots == 0u) continue;       // uniform per type
@@ -207,7 +207,8 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
             if (rexp == 4 || rexp == 2) ra2 = ra2 * ra2;
             racc[p] = ra2;
             if (idx != q.ch[p] && q.ch[p] >= 0) {
-              const float cc = q.rc[p][0] * ra.x + q.rc[p][1] * ra.y + q.rc[p][2] * ra.z;
+              const float4 rc = S.rch[threadIdx.x][p];
+              const float cc = rc.x * ra.x + rc.y * ra.y + rc.z * ra.z;
               // cos on the SFU over [0, pi]; cos(x) = cos(2 pi - x) folds 4 theta / 3.
               const float xr = acos_clamped(cc) * (120.f / 90.f);
               hramp[p] = 0.5f - 0.5f * __cosf(fminf(xr, 6.28318531f - xr));
@@ -277,6 +278,222 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
 
 size_t aff2_smem_bytes(int nmPad) { return tabOffset() + sizeof(float) * (size_t)(kAffRows + 1) * nmPad; }
 
+// The CTA's box in the grid-centred frame, the 8 A cells around it and the
+// calling warp's sub-box in the CTA frame.
+struct Box {
+  double ox, oy, oz;                 // CTA frame origin (its first lattice point)
+  double lo[3], hi[3];               // CTA box
+  int c0[3], ncx, ncy, ncells;       // cells around the box
+  float sblo[3], sbhi[3];            // this warp's sub-box
+  bool warpEmpty;
+};
+
+// Cell ranges of receptor type t in cell group cg: S.cellBeg / S.cellPre.
+// Returns the group's cell count (S.cellPre[ncg] is its atom count).
+__device__ __forceinline__ int cell_prefix(const Aff2Params& P, A2Smem& S, const Box& B, const int t, const int cg) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ncg = min(kCellGroup, B.ncells - cg);
+  __syncthreads();  // the previous group's ranges are no longer read
+  if (warp == 0) {
+    constexpr int kPer = kCellGroup / 32;
+    int cnts[kPer];
+    int mine = 0;
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int i = lane * kPer + u;
+      int cn = 0;
+      if (i < ncg) {
+        const int ci = cg + i;
+        const int cx = B.c0[0] + ci % B.ncx, cy = B.c0[1] + (ci / B.ncx) % B.ncy, cz = B.c0[2] + ci / (B.ncx * B.ncy);
+        const int key = ((cz * P.ncell[1] + cy) * P.ncell[0] + cx) * P.ntypes + t;
+        const int beg = P.ctStart[key];
+        cn = P.ctStart[key + 1] - beg;
+        S.cellBeg[i] = beg;
+      }
+      cnts[u] = cn;
+      mine += cn;
+    }
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    int run = incl - mine;
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int i = lane * kPer + u;
+      if (i < ncg) S.cellPre[i] = run;
+      run += cnts[u];
+    }
+    if (lane == 31) S.cellPre[ncg] = incl;
+  }
+  __syncthreads();
+  return ncg;
+}
+
+// Up to kT atoms v0 .. v0 + kT of the current cell group (type t) that lie
+// within 8 A of the CTA box, appended to the candidate arrays at slot nb
+// (full: with the fields the map sums need).  Returns the new count.
+__device__ __forceinline__ int gather_chunk(const Aff2Params& P, A2Smem& S, const Box& B, const int t, const int ncg,
+                                            const int total, const int v0, const int nb, const bool full) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int v = v0 + tid;
+  bool keep = false;
+  int atom = -1;
+  double4 a = make_double4(0, 0, 0, 0);
+  if (v < total) {
+    int lo_i = 0, hi_i = ncg - 1;  // last cell with cellPre <= v
+    while (lo_i < hi_i) {
+      const int mid = (lo_i + hi_i + 1) >> 1;
+      if (S.cellPre[mid] <= v) lo_i = mid; else hi_i = mid - 1;
+    }
+    atom = P.ctAtoms[S.cellBeg[lo_i] + (v - S.cellPre[lo_i])];
+    a = P.xyz[atom];
+    const double ddx = fmax(fmax(B.lo[0] - a.x, a.x - B.hi[0]), 0.0);
+    const double ddy = fmax(fmax(B.lo[1] - a.y, a.y - B.hi[1]), 0.0);
+    const double ddz = fmax(fmax(B.lo[2] - a.z, a.z - B.hi[2]), 0.0);
+    keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.001;
+  }
+  const unsigned kbal = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) S.cnt[warp] = __popc(kbal);
+  __syncthreads();
+  int tot = 0, off = 0;
+#pragma unroll
+  for (int w = 0; w < kW; w++) {
+    if (w == warp) off = tot;
+    tot += S.cnt[w];
+  }
+  if (keep) {
+    const int j = nb + off + __popc(kbal & ((1u << lane) - 1u));
+    const int inf = P.info[atom];
+    S.pos[j] = make_float4((float)(a.x - B.ox), (float)(a.y - B.oy), (float)(a.z - B.oz), __int_as_float(inf));
+    S.idx[j] = atom;
+    if (full) {
+      S.vs[j] = make_float2(P.vol[atom], P.solq[atom]);
+      S.rvA[j] = make_float4(P.rv[3 * atom], P.rv[3 * atom + 1], P.rv[3 * atom + 2], P.rv2[3 * atom]);
+      S.rvB[j] = make_float2(P.rv2[3 * atom + 1], P.rv2[3 * atom + 2]);
+    }
+  }
+  if (tid == 0) S.typeCount[t] += tot;
+  __syncthreads();
+  return nb + tot;
+}
+
+// Nearest H donor of both points over candidates 0 .. nb (FP64 exact, ties to
+// the lower file index), folded into best / bi.
+template <int NMAX>
+__device__ __forceinline__ void scan_donors(const Aff2Params& P, A2Smem& S, const int nb, double (&best)[2],
+                                            int (&bi)[2], const Pts<NMAX>& q) {
+  __syncthreads();
+  for (int j = 0; j < nb; j++) {
+    const float4 a = S.pos[j];
+    const float dx = a.x - q.px, dy = a.y - q.py;
+    const float dxy = fmaf(dy, dy, dx * dx);
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const float dz = a.z - q.pz[p];
+      const float r2 = fmaf(dz, dz, dxy);
+      if (q.valid[p] && r2 <= (float)best[p] + 1.0e-3f) {
+        const int id = S.idx[j];
+        const double4 a64 = P.xyz[id];
+        const double r64 = rsq64(a64.x, a64.y, a64.z, gcoord(q.ix, P.n2x, P.h), gcoord(q.iy, P.n2y, P.h),
+                                 gcoord(q.iz0 + p, P.n2z, P.h));
+        if (r64 < best[p] || (r64 == best[p] && id < bi[p])) {
+          best[p] = r64;
+          bi[p] = id;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// One batch of nb candidates: per-warp lists, then the types one by one.
+// Returns false if a table copy's bounded wait expired (status set).
+template <int NMAX>
+__device__ __forceinline__ bool process_batch(const Aff2Params& P, A2Smem& S, float* tab, const Box& B, const int nb,
+                                              unsigned& phase, Pts<NMAX>& q) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nmPad = P.nmPad;
+  const unsigned tabBytes = (unsigned)(kAffRows * nmPad * sizeof(float));
+  __syncthreads();  // candidate records and counts are complete
+  if (tid == 0) {
+    int s = 0;
+    for (int t = 0; t < P.ntypes; t++) {
+      S.typeStart[t] = s;
+      s += S.typeCount[t];
+      S.typeCount[t] = 0;
+    }
+    S.typeStart[P.ntypes] = s;
+  }
+  __syncthreads();
+  // This warp's list: the candidates within 8 A of its sub-box (FP32 with margin).
+  int nw = 0;
+  if (!B.warpEmpty)
+    for (int base = 0; base < nb; base += 32) {
+      const int j = base + lane;
+      bool keep = false;
+      if (j < nb) {
+        const float4 a = S.pos[j];
+        const float ddx = fmaxf(fmaxf(B.sblo[0] - a.x, a.x - B.sbhi[0]), 0.f);
+        const float ddy = fmaxf(fmaxf(B.sblo[1] - a.y, a.y - B.sbhi[1]), 0.f);
+        const float ddz = fmaxf(fmaxf(B.sblo[2] - a.z, a.z - B.sbhi[2]), 0.f);
+        keep = fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)) <= 64.01f;
+      }
+      const unsigned b = __ballot_sync(0xffffffffu, keep);
+      if (keep) S.wlist[warp][nw + __popc(b & ((1u << lane) - 1u))] = (unsigned short)j;
+      nw += __popc(b);
+    }
+  __syncwarp();
+  for (int t = lane; t <= P.ntypes; t += 32) {  // first entry of each type (the list is sorted)
+    const int target = S.typeStart[t];
+    int a = 0, b = nw;
+    while (a < b) {
+      const int mid = (a + b) >> 1;
+      if ((int)S.wlist[warp][mid] < target) a = mid + 1; else b = mid;
+    }
+    S.wStart[warp][t] = a;
+  }
+  __syncwarp();
+  for (int t = 0; t < P.ntypes; t++) {
+    if (S.typeStart[t + 1] == S.typeStart[t]) continue;  // uniform
+    if (tid == 0) {
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&S.bar, tabBytes);
+      tma_load_1d(tab, P.table + (size_t)t * kAffRows * nmPad, tabBytes, &S.bar);
+    }
+    if (tid < kMaxMapsPass) {  // read after the __syncthreads_or below
+      const unsigned plain = P.typePlain[t];
+      reinterpret_cast<float*>(S.mask4)[tid] = (plain >> tid) & 1u ? 1.f : 0.f;
+    }
+    const bool ok = mbar_wait_bounded(&S.bar, phase & 1u, P.status);
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) mbar_wait_bounded(&S.bar, phase & 1u, P.status);  // let the copy land before leaving
+      return false;
+    }
+    phase++;
+    const int j0 = S.wStart[warp][t], j1 = S.wStart[warp][t + 1];
+    const unsigned slots = P.typeSlots[t];
+    const unsigned short* wl = S.wlist[warp];
+    const bool ish = (t == P.hydrogen);
+    switch (P.typeAng[t]) {  // uniform
+      case A2_D1:
+        if (ish) run_type<NMAX, A2_D1, true>(P, S, tab, j0, j1, wl, slots, q);
+        else run_type<NMAX, A2_D1, false>(P, S, tab, j0, j1, wl, slots, q);
+        break;
+      case A2_A1: run_type<NMAX, A2_A1, false>(P, S, tab, j0, j1, wl, slots, q); break;
+      case A2_A2: run_type<NMAX, A2_A2, false>(P, S, tab, j0, j1, wl, slots, q); break;
+      default:
+        if (ish) run_type<NMAX, A2_SPH, true>(P, S, tab, j0, j1, wl, slots, q);
+        else run_type<NMAX, A2_SPH, false>(P, S, tab, j0, j1, wl, slots, q);
+        break;
+    }
+    __syncthreads();  // the table buffer is free for the next type
+  }
+  return true;
+}
+
 // One work unit: the CTA block `cta` of job P.  Called once per CTA by
 // affinity2_kernel and repeatedly by the persistent batch kernel.
 template <int NMAX>
@@ -285,7 +502,6 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
   float* tab = reinterpret_cast<float*>(smem_raw + tabOffset());
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int nmPad = P.nmPad;
-  const unsigned tabBytes = (unsigned)(kAffRows * nmPad * sizeof(float));
 
   // This CTA's 8 x 8 x 8 points; this warp's 4 x 4 x 4 sub-box; this thread's two points.
   const int tbx = (P.nx + 7) / 8, tby = (P.ny + 7) / 8;
@@ -298,32 +514,35 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
   q.valid[0] = q.ix < P.nx && q.iy < P.ny && q.iz0 < P.nz;
   q.valid[1] = q.ix < P.nx && q.iy < P.ny && q.iz0 + 1 < P.nz;
   const double h = P.h;
-  const double ox = gcoord(x0, P.n2x, h), oy = gcoord(y0, P.n2y, h), oz = gcoord(z0, P.n2z, h);
-  q.px = (float)(gcoord(q.ix, P.n2x, h) - ox);
-  q.py = (float)(gcoord(q.iy, P.n2y, h) - oy);
-  q.pz[0] = (float)(gcoord(q.iz0, P.n2z, h) - oz);
-  q.pz[1] = (float)(gcoord(q.iz0 + 1, P.n2z, h) - oz);
+  Box B;
+  B.ox = gcoord(x0, P.n2x, h);
+  B.oy = gcoord(y0, P.n2y, h);
+  B.oz = gcoord(z0, P.n2z, h);
+  q.px = (float)(gcoord(q.ix, P.n2x, h) - B.ox);
+  q.py = (float)(gcoord(q.iy, P.n2y, h) - B.oy);
+  q.pz[0] = (float)(gcoord(q.iz0, P.n2z, h) - B.oz);
+  q.pz[1] = (float)(gcoord(q.iz0 + 1, P.n2z, h) - B.oz);
 
   // CTA box (FP64, grid-centred) and the 8 A cells around it.
-  double lo[3], hi[3];
-  lo[0] = ox; hi[0] = gcoord(min(x0 + 8, P.nx) - 1, P.n2x, h);
-  lo[1] = oy; hi[1] = gcoord(min(y0 + 8, P.ny) - 1, P.n2y, h);
-  lo[2] = oz; hi[2] = gcoord(min(z0 + 8, P.nz) - 1, P.n2z, h);
-  int c0[3], c1[3];
+  B.lo[0] = B.ox; B.hi[0] = gcoord(min(x0 + 8, P.nx) - 1, P.n2x, h);
+  B.lo[1] = B.oy; B.hi[1] = gcoord(min(y0 + 8, P.ny) - 1, P.n2y, h);
+  B.lo[2] = B.oz; B.hi[2] = gcoord(min(z0 + 8, P.nz) - 1, P.n2z, h);
+  int c1[3];
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    c0[d] = max(0, (int)floor((lo[d] - 8.0 - P.cellLo[d]) / 8.0));
-    c1[d] = min(P.ncell[d] - 1, (int)floor((hi[d] + 8.0 - P.cellLo[d]) / 8.0));
+    B.c0[d] = max(0, (int)floor((B.lo[d] - 8.0 - P.cellLo[d]) / 8.0));
+    c1[d] = min(P.ncell[d] - 1, (int)floor((B.hi[d] + 8.0 - P.cellLo[d]) / 8.0));
   }
-  const int ncx = c1[0] - c0[0] + 1, ncy = c1[1] - c0[1] + 1, ncz = c1[2] - c0[2] + 1;
-  const int ncells = (ncx > 0 && ncy > 0 && ncz > 0) ? ncx * ncy * ncz : 0;
+  B.ncx = c1[0] - B.c0[0] + 1;
+  B.ncy = c1[1] - B.c0[1] + 1;
+  const int ncz = c1[2] - B.c0[2] + 1;
+  B.ncells = (B.ncx > 0 && B.ncy > 0 && ncz > 0) ? B.ncx * B.ncy * ncz : 0;
 
   // This warp's sub-box in the CTA frame (empty when it lies past the grid edge).
-  const bool warpEmpty = wx >= P.nx || wy >= P.ny || wz >= P.nz;
-  float sblo[3], sbhi[3];
-  sblo[0] = (float)(gcoord(wx, P.n2x, h) - ox); sbhi[0] = (float)(gcoord(min(wx + 3, P.nx - 1), P.n2x, h) - ox);
-  sblo[1] = (float)(gcoord(wy, P.n2y, h) - oy); sbhi[1] = (float)(gcoord(min(wy + 3, P.ny - 1), P.n2y, h) - oy);
-  sblo[2] = (float)(gcoord(wz, P.n2z, h) - oz); sbhi[2] = (float)(gcoord(min(wz + 3, P.nz - 1), P.n2z, h) - oz);
+  B.warpEmpty = wx >= P.nx || wy >= P.ny || wz >= P.nz;
+  B.sblo[0] = (float)(gcoord(wx, P.n2x, h) - B.ox); B.sbhi[0] = (float)(gcoord(min(wx + 3, P.nx - 1), P.n2x, h) - B.ox);
+  B.sblo[1] = (float)(gcoord(wy, P.n2y, h) - B.oy); B.sbhi[1] = (float)(gcoord(min(wy + 3, P.ny - 1), P.n2y, h) - B.oy);
+  B.sblo[2] = (float)(gcoord(wz, P.n2z, h) - B.oz); B.sbhi[2] = (float)(gcoord(min(wz + 3, P.nz - 1), P.n2z, h) - B.oz);
 
   for (int i = tid; i < kAffRows + 1; i += kT) S.sol[i] = i < kAffRows ? P.sol[i] : 0.f;
   for (int i = tid; i < nmPad; i += kT) tab[kAffRows * nmPad + i] = 0.f;
@@ -339,7 +558,6 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
     q.s2[p] = 0.f;
     q.fl[p] = 0u;
     q.ch[p] = -1;
-    q.rc[p][0] = q.rc[p][1] = q.rc[p][2] = 0.f;
 #pragma unroll
     for (int g = 0; g < NMAX / 2; g++) q.em[p][g] = make_float2(0.f, 0.f);
 #pragma unroll
@@ -350,227 +568,52 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
   }
   __syncthreads();
 
-  // Gathers the type-t atoms within 8 A of the box from the cells around it
-  // into the candidate arrays from slot nb on; whenever the next round of up to
-  // kT atoms might not fit, consume() empties the arrays first.
+  // ---- the nearest H donor of both points, from the donors within 8 A of the box ----
   int nb = 0;
-  auto gather = [&](int t, bool full, auto&& consume) -> bool {
-    for (int cg = 0; cg < ncells; cg += kCellGroup) {
-      const int ncg = min(kCellGroup, ncells - cg);
-      __syncthreads();  // the previous group's ranges are no longer read
-      if (warp == 0) {
-        constexpr int kPer = kCellGroup / 32;
-        int cnts[kPer];
-        int mine = 0;
-#pragma unroll
-        for (int u = 0; u < kPer; u++) {
-          const int i = lane * kPer + u;
-          int cn = 0;
-          if (i < ncg) {
-            const int ci = cg + i;
-            const int cx = c0[0] + ci % ncx, cy = c0[1] + (ci / ncx) % ncy, cz = c0[2] + ci / (ncx * ncy);
-            const int key = ((cz * P.ncell[1] + cy) * P.ncell[0] + cx) * P.ntypes + t;
-            const int beg = P.ctStart[key];
-            cn = P.ctStart[key + 1] - beg;
-            S.cellBeg[i] = beg;
-          }
-          cnts[u] = cn;
-          mine += cn;
-        }
-        int incl = mine;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        int run = incl - mine;
-#pragma unroll
-        for (int u = 0; u < kPer; u++) {
-          const int i = lane * kPer + u;
-          if (i < ncg) S.cellPre[i] = run;
-          run += cnts[u];
-        }
-        if (lane == 31) S.cellPre[ncg] = incl;
-      }
-      __syncthreads();
-      const int total = S.cellPre[ncg];
-      for (int v0 = 0; v0 < total; v0 += kT) {
-        if (nb + kT > kCap) {
-          if (!consume()) return false;
-          nb = 0;
-        }
-        const int v = v0 + tid;
-        bool keep = false;
-        int atom = -1;
-        double4 a = make_double4(0, 0, 0, 0);
-        if (v < total) {
-          int lo_i = 0, hi_i = ncg - 1;  // last cell with cellPre <= v
-          while (lo_i < hi_i) {
-            const int mid = (lo_i + hi_i + 1) >> 1;
-            if (S.cellPre[mid] <= v) lo_i = mid; else hi_i = mid - 1;
-          }
-          atom = P.ctAtoms[S.cellBeg[lo_i] + (v - S.cellPre[lo_i])];
-          a = P.xyz[atom];
-          const double ddx = fmax(fmax(lo[0] - a.x, a.x - hi[0]), 0.0);
-          const double ddy = fmax(fmax(lo[1] - a.y, a.y - hi[1]), 0.0);
-          const double ddz = fmax(fmax(lo[2] - a.z, a.z - hi[2]), 0.0);
-          keep = ddx * ddx + ddy * ddy + ddz * ddz <= 64.001;
-        }
-        const unsigned kbal = __ballot_sync(0xffffffffu, keep);
-        if (lane == 0) S.cnt[warp] = __popc(kbal);
-        __syncthreads();
-        int tot = 0, off = 0;
-#pragma unroll
-        for (int w = 0; w < kW; w++) {
-          if (w == warp) off = tot;
-          tot += S.cnt[w];
-        }
-        if (keep) {
-          const int j = nb + off + __popc(kbal & ((1u << lane) - 1u));
-          const int inf = P.info[atom];
-          S.pos[j] = make_float4((float)(a.x - ox), (float)(a.y - oy), (float)(a.z - oz), __int_as_float(inf));
-          S.idx[j] = atom;
-          if (full) {
-            S.vs[j] = make_float2(P.vol[atom], P.solq[atom]);
-            S.rvA[j] = make_float4(P.rv[3 * atom], P.rv[3 * atom + 1], P.rv[3 * atom + 2], P.rv2[3 * atom]);
-            S.rvB[j] = make_float2(P.rv2[3 * atom + 1], P.rv2[3 * atom + 2]);
-          }
-        }
-        if (tid == 0) S.typeCount[t] += tot;
-        nb += tot;
-        __syncthreads();
-      }
-    }
-    return true;
-  };
-
-  // ---- the nearest H donor of both points (FP64 exact, ties to the lower index) ----
   if (P.needClosestH) {
     double best[2] = {1e300, 1e300};
     int bi[2] = {-1, -1};
-    auto scanDonors = [&]() -> bool {
-      __syncthreads();
-      for (int j = 0; j < nb; j++) {
-        const float4 a = S.pos[j];
-        const float dx = a.x - q.px, dy = a.y - q.py;
-        const float dxy = fmaf(dy, dy, dx * dx);
-#pragma unroll
-        for (int p = 0; p < 2; p++) {
-          const float dz = a.z - q.pz[p];
-          const float r2 = fmaf(dz, dz, dxy);
-          if (q.valid[p] && r2 <= (float)best[p] + 1.0e-3f) {
-            const int id = S.idx[j];
-            const double4 a64 = P.xyz[id];
-            const double r64 = rsq64(a64.x, a64.y, a64.z, gcoord(q.ix, P.n2x, h), gcoord(q.iy, P.n2y, h),
-                                     gcoord(q.iz0 + p, P.n2z, h));
-            if (r64 < best[p] || (r64 == best[p] && id < bi[p])) {
-              best[p] = r64;
-              bi[p] = id;
-            }
+    for (int t = 0; t < P.ntypes; t++) {
+      if (!P.typeDonor[t]) continue;
+      for (int cg = 0; cg < B.ncells; cg += kCellGroup) {
+        const int ncg = cell_prefix(P, S, B, t, cg);
+        const int total = S.cellPre[ncg];
+        for (int v0 = 0; v0 < total; v0 += kT) {
+          if (nb + kT > kCap) {
+            scan_donors(P, S, nb, best, bi, q);
+            nb = 0;
           }
+          nb = gather_chunk(P, S, B, t, ncg, total, v0, nb, false);
         }
       }
-      __syncthreads();
-      return true;
-    };
-    for (int t = 0; t < P.ntypes; t++)
-      if (P.typeDonor[t]) gather(t, false, scanDonors);
-    scanDonors();
+    }
+    scan_donors(P, S, nb, best, bi, q);
     nb = 0;
     for (int t = tid; t < kMaxTypes; t += kT) S.typeCount[t] = 0;
 #pragma unroll
     for (int p = 0; p < 2; p++) {
       q.ch[p] = (best[p] <= 64.0) ? bi[p] : -1;
-      if (q.ch[p] >= 0) {
-        q.rc[p][0] = P.rv[3 * q.ch[p]];
-        q.rc[p][1] = P.rv[3 * q.ch[p] + 1];
-        q.rc[p][2] = P.rv[3 * q.ch[p] + 2];
-      }
+      S.rch[tid][p] = q.ch[p] >= 0 ? make_float4(P.rv[3 * q.ch[p]], P.rv[3 * q.ch[p] + 1], P.rv[3 * q.ch[p] + 2], 0.f)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     __syncthreads();
   }
 
-  // ---- map sums: batches of candidates, walked type by type ----
+  // ---- map sums: batches of candidates in type-major order, walked type by type ----
   unsigned phase = 0;
-  bool aborted = false;
-  auto process = [&]() -> bool {
-    __syncthreads();  // candidate records and counts are complete
-    if (tid == 0) {
-      int s = 0;
-      for (int t = 0; t < P.ntypes; t++) {
-        S.typeStart[t] = s;
-        s += S.typeCount[t];
-        S.typeCount[t] = 0;
-      }
-      S.typeStart[P.ntypes] = s;
-    }
-    __syncthreads();
-    // This warp's list: the candidates within 8 A of its sub-box (FP32 with margin).
-    int nw = 0;
-    if (!warpEmpty)
-      for (int base = 0; base < nb; base += 32) {
-        const int j = base + lane;
-        bool keep = false;
-        if (j < nb) {
-          const float4 a = S.pos[j];
-          const float ddx = fmaxf(fmaxf(sblo[0] - a.x, a.x - sbhi[0]), 0.f);
-          const float ddy = fmaxf(fmaxf(sblo[1] - a.y, a.y - sbhi[1]), 0.f);
-          const float ddz = fmaxf(fmaxf(sblo[2] - a.z, a.z - sbhi[2]), 0.f);
-          keep = fmaf(ddz, ddz, fmaf(ddy, ddy, ddx * ddx)) <= 64.01f;
+  for (int t = 0; t < P.ntypes; t++)
+    for (int cg = 0; cg < B.ncells; cg += kCellGroup) {
+      const int ncg = cell_prefix(P, S, B, t, cg);
+      const int total = S.cellPre[ncg];
+      for (int v0 = 0; v0 < total; v0 += kT) {
+        if (nb + kT > kCap) {
+          if (!process_batch(P, S, tab, B, nb, phase, q)) return;
+          nb = 0;
         }
-        const unsigned b = __ballot_sync(0xffffffffu, keep);
-        if (keep) S.wlist[warp][nw + __popc(b & ((1u << lane) - 1u))] = (unsigned short)j;
-        nw += __popc(b);
+        nb = gather_chunk(P, S, B, t, ncg, total, v0, nb, true);
       }
-    __syncwarp();
-    for (int t = lane; t <= P.ntypes; t += 32) {  // first entry of each type (the list is sorted)
-      const int target = S.typeStart[t];
-      int a = 0, b = nw;
-      while (a < b) {
-        const int mid = (a + b) >> 1;
-        if ((int)S.wlist[warp][mid] < target) a = mid + 1; else b = mid;
-      }
-      S.wStart[warp][t] = a;
     }
-    __syncwarp();
-    for (int t = 0; t < P.ntypes; t++) {
-      if (S.typeStart[t + 1] == S.typeStart[t]) continue;  // uniform
-      if (tid == 0) {
-        fence_proxy_async();
-        mbar_arrive_expect_tx(&S.bar, tabBytes);
-        tma_load_1d(tab, P.table + (size_t)t * kAffRows * nmPad, tabBytes, &S.bar);
-      }
-      const bool ok = mbar_wait_bounded(&S.bar, phase & 1u, P.status);
-      if (__syncthreads_or(!ok)) {
-        if (tid == 0) mbar_wait_bounded(&S.bar, phase & 1u, P.status);  // let the copy land before exiting
-        aborted = true;
-        return false;
-      }
-      phase++;
-      const int j0 = S.wStart[warp][t], j1 = S.wStart[warp][t + 1];
-      const unsigned slots = P.typeSlots[t], plain = P.typePlain[t];
-      const unsigned short* wl = S.wlist[warp];
-      const bool ish = (t == P.hydrogen);
-      switch (P.typeAng[t]) {  // uniform
-        case A2_D1:
-          if (ish) run_type<NMAX, A2_D1, true>(P, S, tab, j0, j1, wl, slots, plain, q);
-          else run_type<NMAX, A2_D1, false>(P, S, tab, j0, j1, wl, slots, plain, q);
-          break;
-        case A2_A1: run_type<NMAX, A2_A1, false>(P, S, tab, j0, j1, wl, slots, plain, q); break;
-        case A2_A2: run_type<NMAX, A2_A2, false>(P, S, tab, j0, j1, wl, slots, plain, q); break;
-        default:
-          if (ish) run_type<NMAX, A2_SPH, true>(P, S, tab, j0, j1, wl, slots, plain, q);
-          else run_type<NMAX, A2_SPH, false>(P, S, tab, j0, j1, wl, slots, plain, q);
-          break;
-      }
-      __syncthreads();  // the table buffer is free for the next type
-    }
-    return true;
-  };
-  for (int t = 0; t < P.ntypes && !aborted; t++)
-    if (!gather(t, true, process)) break;
-  if (aborted) return;
-  if (nb > 0 && !process()) return;
+  if (nb > 0 && !process_batch(P, S, tab, B, nb, phase, q)) return;
 
   // ---- results ----
 #pragma unroll
