@@ -126,12 +126,11 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
     const int info = __float_as_int(a.w);
     const bool dis = (info >> 8) & 1;
     if (ISH && dis) continue;        // the reference skips disordered hydrogens (:280); uniform: one candidate
-    const int idx = S.idx[c];
     // Exact 8 A cutoff near the edge.
 #pragma unroll
     for (int p = 0; p < 2; p++)
       if (in[p] && r2[p] > 63.9998f) {
-        const double4 a64 = P.xyz[idx];
+        const double4 a64 = P.xyz[S.idx[c]];
         if (rsq64(a64.x, a64.y, a64.z, gcoord(q.ix, P.n2x, P.h), gcoord(q.iy, P.n2y, P.h),
                   gcoord(q.iz0 + p, P.n2z, P.h)) > 64.0)
           in[p] = false;
@@ -151,7 +150,7 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
         // Within the guard band of a bin edge: the reference's FP64 bin
         // int(100 / (1 / sqrt(r^2))) through the table of r^2 thresholds.
         const int k = min(fr > 0.5f ? b + 1 : b, kAffRows);
-        const double4 a64 = P.xyz[idx];
+        const double4 a64 = P.xyz[S.idx[c]];
         const double r64 = rsq64(a64.x, a64.y, a64.z, gcoord(q.ix, P.n2x, P.h), gcoord(q.iy, P.n2y, P.h),
                                  gcoord(q.iz0 + p, P.n2z, P.h));
         b = (r64 >= P.thr[k]) ? k : k - 1;
@@ -181,6 +180,7 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
     // Directional factors (CalculateGridmaps.cpp:84-197) and the H-bond slots (:199-232).
     float racc[2] = {1.f, 1.f}, rdon[2] = {1.f, 1.f}, hramp[2] = {1.f, 1.f};
     if (ANG != A2_SPH) {
+      const int idx = S.idx[c];
       const float4 ra = S.rvA[c];
       const float2 rb = S.rvB[c];
 #pragma unroll
@@ -579,7 +579,7 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
         const int ncg = cell_prefix(P, S, B, t, cg);
         const int total = S.cellPre[ncg];
         for (int v0 = 0; v0 < total; v0 += kT) {
-          if (nb + kT > kCap) {
+          if (nb + min(kT, total - v0) > kCap) {  // this round keeps at most that many atoms
             scan_donors(P, S, nb, best, bi, q);
             nb = 0;
           }
@@ -606,7 +606,7 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
       const int ncg = cell_prefix(P, S, B, t, cg);
       const int total = S.cellPre[ncg];
       for (int v0 = 0; v0 < total; v0 += kT) {
-        if (nb + kT > kCap) {
+        if (nb + min(kT, total - v0) > kCap) {  // this round keeps at most that many atoms
           if (!process_batch(P, S, tab, B, nb, phase, q)) return;
           nb = 0;
         }
