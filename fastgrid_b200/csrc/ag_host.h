@@ -150,6 +150,7 @@ void precompute(Problem& p, ParamLib& lib, Log& log, double* phaseMs = nullptr);
 // Output
 void writeFld(const Problem& p, const char* programName, Log& log);
 void writeMap(const Problem& p, int mapIndex, Log& log);     // mapIndex in [0, numMaps+2)
+void writeAllMaps(const Problem& p, Log& log);              // every map of the set, formatted and written in parallel
 void writeFloatingGrid(const Problem& p, Log& log);
 std::string mapHeader(const Problem& p);
 double roundOutput(double a);

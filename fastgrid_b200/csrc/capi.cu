@@ -1415,7 +1415,7 @@ extern "C" int ag_batch_free(ag_batch* b) {
 extern "C" int ag_problem_write(ag_problem* P) {
   if (!P || (P->p.out.empty() && !P->p.outView)) return fail(AG_E_INVALID, "no computed maps");
   try {
-    for (int m = 0; m < P->p.numMaps() + 2; m++) ag::writeMap(P->p, m, P->log);
+    ag::writeAllMaps(P->p, P->log);
     ag::writeFloatingGrid(P->p, P->log);
   } catch (ag::ExitProgram& e) {
     return fail(AG_E_HOST, "exit %d: %s", e.code, e.msg.c_str());
@@ -1563,7 +1563,7 @@ int runMain(int argc, char** argv) {
     fprintf(stderr, "Electrostatics performance: %i million atoms/s (whole map set)\n", (int)(pairs / (gpuMs * 1e-3) / 1e6));
   }
   Timer t2;
-  for (int m = 0; m < P.p.numMaps() + 2; m++) ag::writeMap(P.p, m, log);
+  ag::writeAllMaps(P.p, log);
   ag::writeFloatingGrid(P.p, log);
   if (bench) fprintf(stderr, "Saving maps              Real: %.1f ms\n", t2.ms());
 

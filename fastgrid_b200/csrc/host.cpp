@@ -5,6 +5,8 @@
 #include "ag_host.h"
 
 #include <algorithm>
+#include <memory>
+#include <atomic>
 #include <chrono>
 #include <cctype>
 #include <cmath>
@@ -809,6 +811,62 @@ static void writeValuesFile(const std::string& fname, const std::string& header,
   for (int64_t c = 0; c < nchunks; c++)
     if (lens[c] && fwrite(bufs[c].data(), lens[c], 1, f) != 1) log.fatal(-2, "Not enough disk space.");
   if (fclose(f) != 0) log.fatal(-2, "Not enough disk space.");
+}
+
+// Every map file of the set at once: the values of all maps are formatted in
+// parallel chunks (uninitialised buffers), then the files are written in
+// parallel, one thread per file.  Errors are collected and reported after
+// the threads have joined, with the reference's messages.
+void writeAllMaps(const Problem& p, Log& log) {
+  const int nm = p.numMaps();
+  const int nmaps = nm + 2;
+  const int64_t n = p.numPoints;
+  const unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  const int64_t chunk = std::max<int64_t>(1 << 16, (n + nt - 1) / nt);
+  const int64_t nchunks = n ? (n + chunk - 1) / chunk : 0;
+  struct Piece {
+    std::unique_ptr<char[]> buf;
+    size_t len = 0;
+  };
+  std::vector<Piece> pieces((size_t)nmaps * nchunks);
+  std::vector<std::string> names(nmaps);
+  for (int m = 0; m < nmaps; m++) names[m] = m < nm ? p.maps[m].filename : (m == nm ? p.elecFilename : p.desolvFilename);
+  const std::string header = mapHeader(p);
+  std::atomic<int64_t> next(0);
+  auto format = [&] {
+    for (int64_t task; (task = next.fetch_add(1)) < (int64_t)pieces.size();) {
+      const int m = (int)(task / nchunks);
+      if (names[m].empty()) continue;
+      const int64_t c = task % nchunks, b = c * chunk, e = std::min(n, b + chunk);
+      Piece& pc = pieces[(size_t)task];
+      pc.buf.reset(new char[(size_t)(e - b) * 24 + 16]);
+      pc.len = formatValues(p.mapData() + (size_t)m * n + b, e - b, pc.buf.get());
+    }
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; t++) th.emplace_back(format);
+  for (auto& t : th) t.join();
+  th.clear();
+  std::vector<int> err(nmaps, 0);  // 1 cannot open, 2 short write
+  for (int m = 0; m < nmaps; m++) {
+    if (names[m].empty()) continue;
+    th.emplace_back([&, m] {
+      FILE* f = fopen(names[m].c_str(), "w");
+      if (!f) { err[m] = 1; return; }
+      bool ok = fwrite(header.data(), header.size(), 1, f) == 1;
+      for (int64_t c = 0; ok && c < nchunks; c++) {
+        const Piece& pc = pieces[(size_t)m * nchunks + c];
+        if (pc.len) ok = fwrite(pc.buf.get(), pc.len, 1, f) == 1;
+      }
+      if (fclose(f) != 0) ok = false;
+      if (!ok) err[m] = 2;
+    });
+  }
+  for (auto& t : th) t.join();
+  for (int m = 0; m < nmaps; m++) {
+    if (err[m] == 1) log.fatal(-2, "Cannot open grid map \"%s\" for writing.", names[m].c_str());
+    if (err[m] == 2) log.fatal(-2, "Not enough disk space.");
+  }
 }
 
 void writeMap(const Problem& p, int mapIndex, Log& log) {
