@@ -28,6 +28,7 @@
 //    before the map sums need it.
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 #include "ag_device.cuh"
@@ -62,7 +63,12 @@ struct A2Smem {
   float4 mask4[kMaxMapsPass / 4];    // current type: 1 for maps summed plainly, 0 for its H-bond slot maps
   float4 rch[kT][2];                 // per thread and point: rvector of the nearest H donor
   uint64_t bar;
+  // The nearest-donor search keeps each candidate's FP64 record where the map
+  // sums keep vs, rvA and rvB (the two phases do not overlap).
+  __device__ double4* d64() { return reinterpret_cast<double4*>(vs); }
 };
+static_assert(offsetof(A2Smem, vs) % 32 == 0 && offsetof(A2Smem, idx) - offsetof(A2Smem, vs) == kCap * sizeof(double4),
+              "vs, rvA and rvB must hold kCap FP64 records");
 
 __host__ __device__ constexpr size_t tabOffset() { return ((sizeof(A2Smem) + 127) / 128) * 128; }
 
@@ -373,6 +379,8 @@ __device__ __forceinline__ int gather_chunk(const Aff2Params& P, A2Smem& S, cons
       S.vs[j] = make_float2(P.vol[atom], P.solq[atom]);
       S.rvA[j] = make_float4(P.rv[3 * atom], P.rv[3 * atom + 1], P.rv[3 * atom + 2], P.rv2[3 * atom]);
       S.rvB[j] = make_float2(P.rv2[3 * atom + 1], P.rv2[3 * atom + 2]);
+    } else {
+      S.d64()[j] = a;
     }
   }
   if (tid == 0) S.typeCount[t] += tot;
@@ -381,11 +389,15 @@ __device__ __forceinline__ int gather_chunk(const Aff2Params& P, A2Smem& S, cons
 }
 
 // Nearest H donor of both points over candidates 0 .. nb (FP64 exact, ties to
-// the lower file index), folded into best / bi.
+// the lower file index), folded into best / bi.  A first FP32 pass finds each
+// point's smallest r^2 in the batch; the FP64 distance (from the records in
+// shared memory) is formed only for the candidates within 1e-3 A^2 of it,
+// which the FP32 error (< 1e-4 A^2) cannot hide.
 template <int NMAX>
 __device__ __forceinline__ void scan_donors(const Aff2Params& P, A2Smem& S, const int nb, double (&best)[2],
                                             int (&bi)[2], const Pts<NMAX>& q) {
   __syncthreads();
+  float lim[2] = {3.0e38f, 3.0e38f};
   for (int j = 0; j < nb; j++) {
     const float4 a = S.pos[j];
     const float dx = a.x - q.px, dy = a.y - q.py;
@@ -393,10 +405,22 @@ __device__ __forceinline__ void scan_donors(const Aff2Params& P, A2Smem& S, cons
 #pragma unroll
     for (int p = 0; p < 2; p++) {
       const float dz = a.z - q.pz[p];
-      const float r2 = fmaf(dz, dz, dxy);
-      if (q.valid[p] && r2 <= (float)best[p] + 1.0e-3f) {
+      lim[p] = fminf(lim[p], fmaf(dz, dz, dxy));
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < 2; p++) lim[p] = fminf(lim[p], (float)best[p]) + 1.0e-3f;
+  const double4* d64 = S.d64();
+  for (int j = 0; j < nb; j++) {
+    const float4 a = S.pos[j];
+    const float dx = a.x - q.px, dy = a.y - q.py;
+    const float dxy = fmaf(dy, dy, dx * dx);
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const float dz = a.z - q.pz[p];
+      if (q.valid[p] && fmaf(dz, dz, dxy) <= lim[p]) {
         const int id = S.idx[j];
-        const double4 a64 = P.xyz[id];
+        const double4 a64 = d64[j];
         const double r64 = rsq64(a64.x, a64.y, a64.z, gcoord(q.ix, P.n2x, P.h), gcoord(q.iy, P.n2y, P.h),
                                  gcoord(q.iz0 + p, P.n2z, P.h));
         if (r64 < best[p] || (r64 == best[p] && id < bi[p])) {
