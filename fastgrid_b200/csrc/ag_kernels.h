@@ -43,8 +43,7 @@ struct EmapParams {
   float rsmooth2;                 // (100 * rSmooth)^2: atoms this far from the box take the smooth form (0 = off)
   float smoothLam;                // 0.3153767175 / 100: E = exp(-smoothLam * r) with r in 0.01 A
   float smoothK;                  // a + rho = 7.7839 + 66.57180475 / 78.4
-  float smoothD;                  // the fit's range: boxes whose half-diagonal (0.01 A) exceeds it keep the table
-  float2 spoly2[8];               // exp(-smoothLam * u) ~ sum_n spoly2[n] u^n on the box's half-diagonal range
+  float2 spoly2[7];               // exp(-smoothLam * u) ~ sum_n spoly2[n] u^n on the box's half-diagonal range
   int testIdleWait;               // test hook: > 0 adds a wait of that many polls on a barrier nothing arrives on
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1

@@ -370,25 +370,19 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
 
 // Smooth-dielectric class of the e-map: atoms at least rSmooth from a CTA box
 // take invEps(r) = g (1 + (a + rho) E(rc - 0.005) p(r - rc)) with p(u) a
-// degree-7 fit of exp(-lambda u) on [-D, D], D a CTA box half-diagonal (in
-// 0.01 A) that 90% of the boxes do not exceed (larger boxes keep the table
-// path), interpolating at Chebyshev nodes.  The class is off if the fit's
-// relative error exceeds 1e-3.
+// degree-6 fit of exp(-lambda u) on [-D, D], D the largest CTA box
+// half-diagonal (in 0.01 A), interpolating at Chebyshev nodes.  The class is
+// off if the fit's relative error exceeds 1e-3.
 void smoothParams(const ag_ctx* c, agk::EmapParams& P) {
   P.rsmooth2 = 0.f;
   P.smoothLam = (float)(0.3153767175 / 100.0);
   P.smoothK = (float)(7.7839 + 66.57180475 / 78.4);
   if (!c->ddd || !(c->rSmooth > 0.f) || c->hBlocks.empty()) return;
-  // D: the 90th percentile of the CTA boxes' half-diagonals.  Boxes larger than
-  // D (blocks that straddle tiles at the grid edge) keep the table path.
-  std::vector<double> hd;
-  hd.reserve(c->hBlocks.size());
+  double D = 0.0;
   for (const auto& b : c->hBlocks)
-    hd.push_back(std::sqrt((double)b.hx * b.hx + (double)b.hy * b.hy + (double)b.hz * b.hz));
-  std::sort(hd.begin(), hd.end());
-  const double D = hd[(hd.size() * 9) / 10];
+    D = std::max(D, std::sqrt((double)b.hx * b.hx + (double)b.hy * b.hy + (double)b.hz * b.hz));
   const double lam = 0.3153767175 / 100.0;
-  constexpr int kDeg = 7;
+  constexpr int kDeg = 6;
   // Interpolate f(t) = exp(-lam D t) at the Chebyshev nodes of [-1, 1] (Newton divided differences),
   // then expand to monomials in t and rescale to u = D t.
   double x[kDeg + 1], dd[kDeg + 1];
@@ -423,7 +417,6 @@ void smoothParams(const ag_ctx* c, agk::EmapParams& P) {
   }
   if (!(worst < 1e-3)) return;
   for (int k = 0; k <= kDeg; k++) P.spoly2[k] = make_float2(cf[k], cf[k]);
-  P.smoothD = (float)D;
   P.rsmooth2 = (100.f * c->rSmooth) * (100.f * c->rSmooth);
 }
 

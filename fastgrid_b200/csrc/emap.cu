@@ -29,7 +29,7 @@
 //        reference's 0.01 A bin (the step from bin to bin is then a zero-mean
 //        residual below 2.2e-7 of the term), as E(r) = E(rc) p(r - rc): rc is
 //        the atom's distance to the CTA box centre (one expf per atom and CTA)
-//        and p a degree-7 polynomial of exp(-lambda u) on the box's
+//        and p a degree-6 polynomial of exp(-lambda u) on the box's
 //        half-diagonal range, fitted on the host (relative error < 1e-3, so
 //        < 1.4e-7 of the term for rSmooth >= 35 A);
 //      far (d >= rFar, at least 50 A): the table has saturated there (its
@@ -218,8 +218,7 @@ __device__ __forceinline__ void smooth_atoms(const float4* __restrict__ list, co
         const float2 r2 = __ffma2_rn(dx, dx, dyz2);
         const float2 rs = rsqrt2(r2);
         const float2 u = __ffma2_rn(r2, rs, nrc);  // r - rc (scaled by 100)
-        float2 pp = __ffma2_rn(u, P.spoly2[7], P.spoly2[6]);
-        pp = __ffma2_rn(u, pp, P.spoly2[5]);
+        float2 pp = __ffma2_rn(u, P.spoly2[6], P.spoly2[5]);
         pp = __ffma2_rn(u, pp, P.spoly2[4]);
         pp = __ffma2_rn(u, pp, P.spoly2[3]);
         pp = __ffma2_rn(u, pp, P.spoly2[2]);
@@ -299,9 +298,6 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
 #pragma unroll
   for (int k = 0; k < kNX / 2; k++) { sum[k] = make_float2(0.f, 0.f); cmp[k] = make_float2(0.f, 0.f); }
 
-  // The smooth class needs every point of the box within the fit's range of the box centre.
-  const float rsmooth2 =
-      (P.rsmooth2 > 0.f && sqrtf(B.hx * B.hx + B.hy * B.hy + B.hz * B.hz) <= P.smoothD) ? P.rsmooth2 : 0.f;
   const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
   const float kBias = 8388608.f;  // 2^23: adding it with round-down leaves floor() in the low bits
 
@@ -345,7 +341,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
                   dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
       const float d2 = dx * dx + dy * dy + dz * dz;
-      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? ((rsmooth2 > 0.f && d2 >= rsmooth2) ? 3 : 1) : 2);
+      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? ((P.rsmooth2 > 0.f && d2 >= P.rsmooth2) ? 3 : 1) : 2);
       if (cls == 2) loc.w *= gFar;
       if (cls == 3) {
         const float rc = sqrtf(fmaf(loc.z, loc.z, fmaf(loc.y, loc.y, loc.x * loc.x)));
