@@ -99,7 +99,6 @@ struct ag_ctx {
   std::vector<float> solparProbe, volProbe;
   int emapMode = agk::kEmapKahan;
   float rNear = 11.0f;
-  float rSmooth = 40.0f;      // A: mid atoms at least this far from the CTA box take the smooth dielectric (0 = off)
   float delta = 2.0e-3f;
   int anaPairs = 0;  // of each thread's 4 point pairs, those evaluating mid atoms' dielectric analytically
                      // (none: measured fastest on B200, the analytic pairs' ex2 and series cost more than the

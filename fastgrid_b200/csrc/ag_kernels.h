@@ -40,10 +40,6 @@ struct EmapParams {
   float2 negBias2;                // -2^23, both halves: bin = f + negBias2
   float2 negLambda2;              // -0.3153767175 / 100 / ln 2, both halves: E = 2^(negLambda2 * bin)
   float2 poly2[6];                // invEps(bin) = sum_n poly2[n] E^n (both halves equal) for E <= 0.031
-  float rsmooth2;                 // (100 * rSmooth)^2: atoms this far from the box take the smooth form (0 = off)
-  float smoothLam;                // 0.3153767175 / 100: E = exp(-smoothLam * r) with r in 0.01 A
-  float smoothK;                  // a + rho = 7.7839 + 66.57180475 / 78.4
-  float2 spoly2[7];               // exp(-smoothLam * u) ~ sum_n spoly2[n] u^n on the box's half-diagonal range
   int testIdleWait;               // test hook: > 0 adds a wait of that many polls on a barrier nothing arrives on
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1

@@ -190,10 +190,6 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "tcgen05 switch must be 0 or 1");
       agc::surrUseTc(c, v != 0.0);
       return AG_OK;
-    case AG_TUNE_EMAP_SMOOTH_FROM:
-      if (!(v == 0.0 || (v >= 35.0 && v <= 50.0))) return fail(AG_E_INVALID, "smooth-dielectric radius must be 0 or in [35, 50] A");
-      c->rSmooth = (float)v;
-      return AG_OK;
     case AG_TUNE_AFFINITY_KERNEL:
       if (!(v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "affinity kernel must be 1 or 2");
       c->affKernel = (int)v;
@@ -368,58 +364,6 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
   return AG_OK;
 }
 
-// Smooth-dielectric class of the e-map: atoms at least rSmooth from a CTA box
-// take invEps(r) = g (1 + (a + rho) E(rc - 0.005) p(r - rc)) with p(u) a
-// degree-6 fit of exp(-lambda u) on [-D, D], D the largest CTA box
-// half-diagonal (in 0.01 A), interpolating at Chebyshev nodes.  The class is
-// off if the fit's relative error exceeds 1e-3.
-void smoothParams(const ag_ctx* c, agk::EmapParams& P) {
-  P.rsmooth2 = 0.f;
-  P.smoothLam = (float)(0.3153767175 / 100.0);
-  P.smoothK = (float)(7.7839 + 66.57180475 / 78.4);
-  if (!c->ddd || !(c->rSmooth > 0.f) || c->hBlocks.empty()) return;
-  double D = 0.0;
-  for (const auto& b : c->hBlocks)
-    D = std::max(D, std::sqrt((double)b.hx * b.hx + (double)b.hy * b.hy + (double)b.hz * b.hz));
-  const double lam = 0.3153767175 / 100.0;
-  constexpr int kDeg = 6;
-  // Interpolate f(t) = exp(-lam D t) at the Chebyshev nodes of [-1, 1] (Newton divided differences),
-  // then expand to monomials in t and rescale to u = D t.
-  double x[kDeg + 1], dd[kDeg + 1];
-  for (int i = 0; i <= kDeg; i++) {
-    x[i] = std::cos((2.0 * i + 1.0) * M_PI / (2.0 * (kDeg + 1)));
-    dd[i] = std::exp(-lam * D * x[i]);
-  }
-  for (int j = 1; j <= kDeg; j++)
-    for (int i = kDeg; i >= j; i--) dd[i] = (dd[i] - dd[i - 1]) / (x[i] - x[i - j]);
-  double mono[kDeg + 1] = {0};   // coefficients of the Newton form expanded, in t
-  double basis[kDeg + 1] = {1};  // product (t - x0) ... (t - x_{j-1}) as monomials
-  for (int j = 0; j <= kDeg; j++) {
-    for (int k = 0; k <= j; k++) mono[k] += dd[j] * basis[k];
-    if (j < kDeg) {
-      double nb[kDeg + 1] = {0};
-      for (int k = 0; k <= j; k++) {
-        nb[k + 1] += basis[k];
-        nb[k] -= x[j] * basis[k];
-      }
-      for (int k = 0; k <= kDeg; k++) basis[k] = nb[k];
-    }
-  }
-  float cf[kDeg + 1];
-  double scale = 1.0;
-  for (int k = 0; k <= kDeg; k++, scale /= D) cf[k] = (float)(mono[k] * scale);
-  double worst = 0.0;
-  for (int i = 0; i <= 4000; i++) {  // the fit as the kernel evaluates it (FP32 Horner)
-    const float u = (float)(-D + 2.0 * D * i / 4000.0);
-    float pp = cf[kDeg];
-    for (int k = kDeg - 1; k >= 0; k--) pp = std::fma(u, pp, cf[k]);
-    worst = std::max(worst, std::fabs((double)pp / std::exp(-lam * (double)u) - 1.0));
-  }
-  if (!(worst < 1e-3)) return;
-  for (int k = 0; k <= kDeg; k++) P.spoly2[k] = make_float2(cf[k], cf[k]);
-  P.rsmooth2 = (100.f * c->rSmooth) * (100.f * c->rSmooth);
-}
-
 // Launch parameters of the e-map of the staged job; allowSplit = false keeps
 // every CTA on all atoms (the batch kernel's mode).
 int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P) {
@@ -455,7 +399,6 @@ int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P)
     P.negBias2 = make_float2(-8388608.f, -8388608.f);
     P.anaPairs = c->anaPairs;
   }
-  smoothParams(c, P);
   P.out = dOut;
   P.status = c->status.p;
   P.testIdleWait = c->testIdleWait;

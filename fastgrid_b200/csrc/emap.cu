@@ -19,24 +19,12 @@
 //      near (d < rNear): 1/r capped at 2, Kahan-compensated per pair, and the
 //        bin decided exactly in FP64 (squared-distance threshold table) when
 //        100 r lies within `delta` of a bin edge;
-//      mid (rNear <= d < rSmooth): bin by a round-down FMA, table read;
-//      smooth (rSmooth <= d < rFar, when rSmooth > 0): no table read.  There
-//        the dielectric is within 1.4e-4 of saturation and varies smoothly:
-//        invEps(r) = g (1 + (a + rho) E(r)) up to O(E^2) < 2e-9, with
-//        E(r) = exp(-0.3153767175 r), g = invEps[8191], a = 7.7839,
-//        rho = 66.57180475 / 78.4 (the rational form of autogrid.h:233-239
-//        expanded in E).  E is taken at r - 0.005 A, the middle of the
-//        reference's 0.01 A bin (the step from bin to bin is then a zero-mean
-//        residual below 2.2e-7 of the term), as E(r) = E(rc) p(r - rc): rc is
-//        the atom's distance to the CTA box centre (one expf per atom and CTA)
-//        and p a degree-6 polynomial of exp(-lambda u) on the box's
-//        half-diagonal range, fitted on the host (relative error < 1e-3, so
-//        < 1.4e-7 of the term for rSmooth >= 35 A);
+//      mid (rNear <= d < rFar): bin by a round-down FMA, table read;
 //      far (d >= rFar, at least 50 A): the table has saturated there (its
 //        entries differ from entry 8191 by < 2e-6 relative), so the term is
 //        w * invEps[8191] / r with no table read.
-//    Mid, smooth and far terms are summed in plain FP32 over chunks of kChunk
-//    atoms and the chunk sums are Kahan-compensated.
+//    Mid and far terms are summed in plain FP32 over chunks of kChunk atoms
+//    and the chunk sums are Kahan-compensated.
 //  * When the grid is too small to fill the GPU, atoms are split across CTAs
 //    and the per-CTA results are reduced in FP64, in a fixed order, by a
 //    second kernel.
@@ -62,10 +50,8 @@ struct EmapSmem {
   float4 nearA[kTile];            // local scaled x, y, z and 100*w
   float4 midA[kTile];             // mid atoms, table read
   float4 farA[kTile];             // w pre-multiplied by invEps[8191]
-  float4 smA[kTile];              // smooth atoms: x, y, z, w * invEps[8191]
-  float2 smE[kTile];              // smooth atoms: rc (distance to the box centre), w * invEps[8191] (a + rho) E(rc - 0.005 A)
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
-  int cnt[4][kThreads / 32];
+  int cnt[3][kThreads / 32];
   double wpart[kThreads / 32];
   int unit;                       // persistent batch kernel: the unit being processed
   uint64_t bar[2];
@@ -192,45 +178,6 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
   }
 }
 
-// Smooth-list atoms: no bin and no table read; the dielectric factor is
-// (w g) + (w g (a + rho) E(rc - 0.005)) p(r - rc), p on the FMA pipe.
-template <int MODE>
-__device__ __forceinline__ void smooth_atoms(const float4* __restrict__ list, const float2* __restrict__ extra, int n,
-                                             const float2 (&gxn)[kNX / 2], float gy, float gz,
-                                             float2 (&sum)[kNX / 2], float2 (&cmp)[kNX / 2], const EmapParams& P) {
-#pragma unroll 1
-  for (int j0 = 0; j0 < n; j0 += kChunk) {
-    float2 cs[kNX / 2];
-#pragma unroll
-    for (int k = 0; k < kNX / 2; k++)
-      cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : sum[k];
-    const int j1 = min(n, j0 + kChunk);
-#pragma unroll 4
-    for (int j = j0; j < j1; j++) {
-      const float4 a = list[j];
-      const float2 e = extra[j];
-      const float dy = a.y - gy, dz = a.z - gz;
-      const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy));
-      const float2 ax = dup2(a.x), wg = dup2(a.w), wA = dup2(e.y), nrc = dup2(-e.x);
-#pragma unroll
-      for (int k = 0; k < kNX / 2; k++) {
-        const float2 dx = __fadd2_rn(ax, gxn[k]);
-        const float2 r2 = __ffma2_rn(dx, dx, dyz2);
-        const float2 rs = rsqrt2(r2);
-        const float2 u = __ffma2_rn(r2, rs, nrc);  // r - rc (scaled by 100)
-        float2 pp = __ffma2_rn(u, P.spoly2[6], P.spoly2[5]);
-        pp = __ffma2_rn(u, pp, P.spoly2[4]);
-        pp = __ffma2_rn(u, pp, P.spoly2[3]);
-        pp = __ffma2_rn(u, pp, P.spoly2[2]);
-        pp = __ffma2_rn(u, pp, P.spoly2[1]);
-        pp = __ffma2_rn(u, pp, P.spoly2[0]);
-        cs[k] = __ffma2_rn(rs, __ffma2_rn(wA, pp, wg), cs[k]);
-      }
-    }
-    add_chunk<MODE>(sum, cmp, cs);
-  }
-}
-
 template <int MODE, bool CLAMP>
 __device__ __forceinline__ void mid_atoms_any(const float4* __restrict__ list, uint32_t tabBiased, int n,
                                               const float2 (&gxn)[kNX / 2], float gy, float gz, float2 (&sum)[kNX / 2],
@@ -328,9 +275,8 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     }
 
     // Classify and convert this tile's atoms (one atom per thread).
-    int cls = -1;  // 0 near, 1 mid, 2 far, 3 smooth
+    int cls = -1;  // 0 near, 1 mid, 2 far
     float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
-    float2 sme = make_float2(0.f, 0.f);
     if (tid < nt) {
       double4 a = S.ring[slot][tid];
       wsum += a.w;
@@ -341,33 +287,25 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
                   dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
       const float d2 = dx * dx + dy * dy + dz * dz;
-      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? ((P.rsmooth2 > 0.f && d2 >= P.rsmooth2) ? 3 : 1) : 2);
+      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? 1 : 2);
       if (cls == 2) loc.w *= gFar;
-      if (cls == 3) {
-        const float rc = sqrtf(fmaf(loc.z, loc.z, fmaf(loc.y, loc.y, loc.x * loc.x)));
-        loc.w *= gFar;
-        sme = make_float2(rc, loc.w * P.smoothK * expf(-P.smoothLam * (rc - 0.5f)));
-      }
     }
     const unsigned b0 = __ballot_sync(0xffffffffu, cls == 0);
     const unsigned b1 = __ballot_sync(0xffffffffu, cls == 1);
     const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-    const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
     if (lane == 0) {
       S.cnt[0][warp] = __popc(b0);
       S.cnt[1][warp] = __popc(b1);
       S.cnt[2][warp] = __popc(b2);
-      S.cnt[3][warp] = __popc(b3);
     }
     __syncthreads();
-    int nNear = 0, nMid = 0, nFar = 0, nSm = 0, off0 = 0, off1 = 0, off2 = 0, off3 = 0;
+    int nNear = 0, nMid = 0, nFar = 0, off0 = 0, off1 = 0, off2 = 0;
 #pragma unroll
     for (int w = 0; w < kThreads / 32; w++) {
-      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; off3 = nSm; }
+      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; }
       nNear += S.cnt[0][w];
       nMid += S.cnt[1][w];
       nFar += S.cnt[2][w];
-      nSm += S.cnt[3][w];
     }
     const unsigned lt = (1u << lane) - 1u;
     if (cls == 0) {
@@ -378,10 +316,6 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       S.midA[off1 + __popc(b1 & lt)] = loc;
     } else if (cls == 2) {
       S.farA[off2 + __popc(b2 & lt)] = loc;
-    } else if (cls == 3) {
-      const int pos = off3 + __popc(b3 & lt);
-      S.smA[pos] = loc;
-      S.smE[pos] = sme;
     }
     __syncthreads();
 
@@ -393,9 +327,6 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       else
         mid_atoms_any<MODE, false>(S.midA, tabBiased, nMid, gxn, gy, gz, sum, cmp, P);
     }
-
-    // Smooth atoms: the dielectric's smooth form, no table.
-    if (DDD && nSm > 0) smooth_atoms<MODE>(S.smA, S.smE, nSm, gxn, gy, gz, sum, cmp, P);
 
     // Far atoms: saturated dielectric (or the constant dielectric), no table.
 #pragma unroll 1

@@ -97,8 +97,6 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
                                          neighbouring lanes sharing a 16-point x span alternately (default 2) */
 #define AG_TUNE_EMAP_TILE 5           /* direct e-map: TX*10000 + TY*100 + TZ work items per CTA tile, product 256 (default 20816) */
 #define AG_TUNE_SURROGATE_TCGEN05 6   /* 0/1: surrogate corrector convolutions on tcgen05 (1, default) or mma.sync (0) */
-#define AG_TUNE_EMAP_SMOOTH_FROM 10   /* A, 0 or 35..50: e-map atoms at least this far from a CTA box take the
-                                         dielectric's smooth form instead of a table read (default 40; 0 = off) */
 #define AG_TUNE_AFFINITY_KERNEL 9     /* affinity pass: 2 two grid points per thread, type-major candidates,
                                          nearest donor found in the kernel (default); 1 one point per thread
                                          with a separate nearest-donor kernel (also used for passes with more

@@ -112,34 +112,6 @@ def test_many_hbond_maps(tmp_path):
         assert (np.abs(gpu[p.n_maps + 1] - od) <= np.maximum(AFF_ABS, AFF_REL * np.abs(od))).all(), k
 
 
-def test_emap_smooth_dielectric_class(tmp_path):
-    """Atoms 35-50 A or more from a CTA box take the dielectric's smooth form
-    (no table read).  On a grid whose corners lie far from the receptor, the
-    e-map with the class at 35 A, at 40 A (the default) and off must all match
-    the FP64 oracle within 1e-4, and each other within 2e-5."""
-    fg.synth_write(str(tmp_path), "sm", n_atoms=6000, semi_axes=(22, 20, 18), npts=150, seed=23,
-                   ligand_types="C")
-    with chdir(str(tmp_path)):
-        p = fg.Problem("sm.gpf", log="sm.glg")
-    x, eps = p.xyzw(), p.inv_eps()
-    maps = {}
-    for r in (35, 40, 0):
-        c = fg.Context(0)
-        try:
-            c.tune(fg.AG_TUNE_EMAP_SMOOTH_FROM, r)
-            maps[r] = c.emap(p.grid, x, eps).astype(np.float64)
-        finally:
-            c.close()
-    rng = np.random.default_rng(9)
-    idx = np.unique(np.concatenate([rng.choice(p.npoints, 2500, replace=False),
-                                    np.arange(0, p.npoints, p.npoints // 500)]))
-    ref = oracle.emap_points(p.grid, x, eps, idx)
-    for r, m in maps.items():
-        assert np.abs(m[idx] - ref).max() <= E_TOL, (r, np.abs(m[idx] - ref).max())
-    assert np.abs(maps[35] - maps[0]).max() <= 2e-5
-    assert np.abs(maps[40] - maps[0]).max() <= 2e-5
-
-
 def test_emap_edge_cases(ctx):
     """Atoms on a grid point, within 0.01 A of one, at r = 0.5 A (the 1/r cap),
     beyond 81.91 A (the table clamp), and grids that are not multiples of the
