@@ -208,3 +208,17 @@ def test_cli_timeout_ends_a_stalled_job(tmp_path):
     assert r.returncode == 0
     assert "Timeout! Process terminated." in r.stderr
     assert 0.9 <= dt < 20
+
+
+def test_shipped_surrogate_weights_match_their_training_report():
+    """fastgrid_b200/surrogate_weights.bin was written by the training run whose
+    report (command, seed, loss per epoch, timings, GPU) is
+    fastgrid_b200/surrogate_weights.json; the report's SHA-256 pins the file."""
+    import hashlib
+    import json
+    rep = json.load(open(os.path.join(REPO, "fastgrid_b200", "surrogate_weights.json")))
+    data = open(fg.DEFAULT_WEIGHTS, "rb").read()
+    assert hashlib.sha256(data).hexdigest() == rep["weights_sha256"]
+    assert rep["receptors"] == 200 and rep["epochs"] == 10 and len(rep["loss_per_epoch"]) == 10
+    assert rep["last_epoch_loss"] < 0.1 * rep["first_epoch_loss"]
+    assert rep["command"].startswith("python -m fastgrid_b200.train_surrogate")
