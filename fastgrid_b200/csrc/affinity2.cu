@@ -16,10 +16,11 @@
 //    segments, file order inside each), so a batch arrives sorted by receptor
 //    type without a sort, and each type's table rows are loaded once per batch
 //    (one TMA bulk copy);
-//  * the plain map sums add whole table rows with packed FP32x2 FMAs
-//    multiplied by a per-type 0/1 mask; the mask removes the maps whose H-bond
-//    term applies to that type (the "slots", at most four per pass), which
-//    read their table entry separately;
+//  * the plain map sums add whole table rows with packed FP32x2 adds (types
+//    without an H-bond term) or FMAs with a per-type 0/1 mask; the mask removes
+//    the maps whose H-bond term applies to that type (the "slots", at most four
+//    per pass), which read their table entry separately; a spare column of the
+//    row carries the desolvation value;
 //  * a point beyond 8 A of the atom reads an all-zero extra table row, so the
 //    plain sums need no branch;
 //  * the nearest H donor of each point (the reference's kd-tree query,
@@ -107,7 +108,7 @@ __device__ __forceinline__ double gcoord(int i, int n2, double h) { return __dmu
 
 // One receptor type's candidates in this warp's list, for both points.
 // ANG: angular class of the type; ISH: the type is "HD" (disordered ones are skipped).
-template <int NMAX, int ANG, bool ISH>
+template <int NMAX, int ANG, bool ISH, bool PLAIN>
 __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, const float* tab, const int j0,
                                          const int j1, const unsigned short* wl, const unsigned slots,
                                          Pts<NMAX>& q) {
@@ -163,25 +164,37 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
       }
       iR[p] = in[p] ? min(max(b, 0), kAffRows - 1) : kAffRows;  // kAffRows: the zero row
     }
-    const float2 v = S.vs[c];
-#pragma unroll
-    for (int p = 0; p < 2; p++) {
-      const float sv = S.sol[iR[p]];
-      q.s1[p] = fmaf(sv, v.x, q.s1[p]);
-      q.s2[p] = fmaf(sv, v.y, q.s2[p]);
-    }
+    // Plain map sums: whole rows.  PLAIN (no H-bond slot applies to this type)
+    // adds them directly, otherwise through the type's 0/1 mask.  When the pass
+    // has a spare column the row's last entry holds the desolvation value.
+    float solv[2] = {0.f, 0.f};
+    const int lastQ = rowQ - 1;
 #pragma unroll
     for (int g4 = 0; g4 < NMAX / 4; g4++) {
       if (4 * g4 >= P.nmaps) break;
-      const float4 m4 = S.mask4[g4];  // same address in every lane: one broadcast for both points
+      float4 m4 = make_float4(1.f, 1.f, 1.f, 1.f);
+      if (!PLAIN) m4 = S.mask4[g4];  // same address in every lane: one broadcast for both points
 #pragma unroll
       for (int p = 0; p < 2; p++) {
         const float4 e4 = tab4[iR[p] * rowQ + g4];
-        q.em[p][2 * g4] = __ffma2_rn(make_float2(e4.x, e4.y), make_float2(m4.x, m4.y), q.em[p][2 * g4]);
-        q.em[p][2 * g4 + 1] = __ffma2_rn(make_float2(e4.z, e4.w), make_float2(m4.z, m4.w), q.em[p][2 * g4 + 1]);
+        if (PLAIN) {
+          q.em[p][2 * g4] = __fadd2_rn(q.em[p][2 * g4], make_float2(e4.x, e4.y));
+          q.em[p][2 * g4 + 1] = __fadd2_rn(q.em[p][2 * g4 + 1], make_float2(e4.z, e4.w));
+        } else {
+          q.em[p][2 * g4] = __ffma2_rn(make_float2(e4.x, e4.y), make_float2(m4.x, m4.y), q.em[p][2 * g4]);
+          q.em[p][2 * g4 + 1] = __ffma2_rn(make_float2(e4.z, e4.w), make_float2(m4.z, m4.w), q.em[p][2 * g4 + 1]);
+        }
+        if (g4 == lastQ) solv[p] = e4.w;
       }
     }
-    if (slots == 0u) continue;       // uniform per type
+    const float2 v = S.vs[c];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const float sv = P.solInRow ? solv[p] : S.sol[iR[p]];
+      q.s1[p] = fmaf(sv, v.x, q.s1[p]);
+      q.s2[p] = fmaf(sv, v.y, q.s2[p]);
+    }
+    if (PLAIN) continue;
 
     // Directional factors (CalculateGridmaps.cpp:84-197) and the H-bond slots (:199-232).
     float racc[2] = {1.f, 1.f}, rdon[2] = {1.f, 1.f}, hramp[2] = {1.f, 1.f};
@@ -501,17 +514,22 @@ __device__ __forceinline__ bool process_batch(const Aff2Params& P, A2Smem& S, fl
     const unsigned slots = P.typeSlots[t];
     const unsigned short* wl = S.wlist[warp];
     const bool ish = (t == P.hydrogen);
-    switch (P.typeAng[t]) {  // uniform
-      case A2_D1:
-        if (ish) run_type<NMAX, A2_D1, true>(P, S, tab, j0, j1, wl, slots, q);
-        else run_type<NMAX, A2_D1, false>(P, S, tab, j0, j1, wl, slots, q);
-        break;
-      case A2_A1: run_type<NMAX, A2_A1, false>(P, S, tab, j0, j1, wl, slots, q); break;
-      case A2_A2: run_type<NMAX, A2_A2, false>(P, S, tab, j0, j1, wl, slots, q); break;
-      default:
-        if (ish) run_type<NMAX, A2_SPH, true>(P, S, tab, j0, j1, wl, slots, q);
-        else run_type<NMAX, A2_SPH, false>(P, S, tab, j0, j1, wl, slots, q);
-        break;
+    if (slots == 0u) {  // uniform: no H-bond term, no angular factors
+      if (ish) run_type<NMAX, A2_SPH, true, true>(P, S, tab, j0, j1, wl, slots, q);
+      else run_type<NMAX, A2_SPH, false, true>(P, S, tab, j0, j1, wl, slots, q);
+    } else {
+      switch (P.typeAng[t]) {  // uniform
+        case A2_D1:
+          if (ish) run_type<NMAX, A2_D1, true, false>(P, S, tab, j0, j1, wl, slots, q);
+          else run_type<NMAX, A2_D1, false, false>(P, S, tab, j0, j1, wl, slots, q);
+          break;
+        case A2_A1: run_type<NMAX, A2_A1, false, false>(P, S, tab, j0, j1, wl, slots, q); break;
+        case A2_A2: run_type<NMAX, A2_A2, false, false>(P, S, tab, j0, j1, wl, slots, q); break;
+        default:
+          if (ish) run_type<NMAX, A2_SPH, true, false>(P, S, tab, j0, j1, wl, slots, q);
+          else run_type<NMAX, A2_SPH, false, false>(P, S, tab, j0, j1, wl, slots, q);
+          break;
+      }
     }
     __syncthreads();  // the table buffer is free for the next type
   }

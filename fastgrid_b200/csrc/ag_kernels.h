@@ -172,6 +172,7 @@ struct Aff2Params {
   const float* table;             // [ntypes][kAffRows][nmPad] FP32
   const float* tableH;            // [kAffRows][nmPad] rows of the "HD" type, or null
   const float* sol;               // kAffRows
+  int solInRow;                   // the table rows' last column (nmPad - 1 >= nmaps) holds sol
   const double* thr;              // affinity bin thresholds (kAffRows + 1)
   float delta;                    // guard half-width around bin edges (bins)
   int needClosestH;               // some D1 type meets an acceptor-probe slot: find the nearest donor

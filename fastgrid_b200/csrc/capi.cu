@@ -12,6 +12,7 @@
 #include <mutex>
 #include <signal.h>
 #include <string>
+#include <thread>
 #include <sys/wait.h>
 #include <unistd.h>
 #include <vector>
@@ -534,10 +535,13 @@ int stageAffinity(ag_ctx* c, const ag_receptor* r, const ag_affinity_params* p) 
   std::vector<float> tab(std::max<size_t>(tabSize, 4), 0.f), tabH(std::max<size_t>(tabHSize, 4), 0.f);
   for (auto& ps : c->passes) {
     for (int t = 0; t < nt; t++)
-      for (int i = 0; i < agk::kAffRows; i++)
+      for (int i = 0; i < agk::kAffRows; i++) {
         for (int g = 0; g < ps.nm; g++)
           tab[ps.tabOff + ((size_t)t * agk::kAffRows + i) * ps.nmPad + g] =
               (float)p->energy[((size_t)t * 8192 + i) * nm + ps.m0 + g];
+        // A spare last column carries the desolvation value (read by the two-point kernel).
+        if (ps.nm < ps.nmPad) tab[ps.tabOff + ((size_t)t * agk::kAffRows + i) * ps.nmPad + ps.nmPad - 1] = (float)p->sol[i];
+      }
     if (p->hydrogen >= 0 && p->hydrogen < nt)
       for (int i = 0; i < agk::kAffRows; i++)
         for (int g = 0; g < ps.nm; g++)
@@ -675,6 +679,7 @@ int buildAff2Params(ag_ctx* c, float* dMaps, float* dDmap, std::vector<agk::Aff2
     P.table = c->affTab.p + ps.tabOff;
     P.tableH = (c->hydrogen >= 0 && c->hydrogen < nt) ? c->affTabH.p + ps.tabHOff : nullptr;
     P.sol = c->sol.p;
+    P.solInRow = ps.nm < ps.nmPad ? 1 : 0;
     P.thr = c->thrA.p;
     P.delta = 1.0e-3f;
     if (!passSlots(c, ps, P.nslots, P.slotMap, P.slotKind)) return fail(AG_E_INVALID, "too many H-bond maps");
@@ -1464,6 +1469,23 @@ int runMain(int argc, char** argv) {
   log.open(logf.c_str());
   log.print("%s 4.2.1 (B200 map engine)\n\n", prog);
   ag::ParamLib lib(v4);
+  // The CUDA context (the longest host step) is created on a second thread
+  // while this one parses the inputs and builds the tables.
+  struct CtxStart {
+    ag_ctx* ctx = nullptr;
+    int rc = AG_OK;
+    std::string err;
+    std::thread th;
+    ~CtxStart() {  // also on the error paths of the host steps
+      if (th.joinable()) th.join();
+      if (ctx) ag_ctx_destroy(ctx);
+    }
+  } cs;
+  Timer tc;
+  cs.th = std::thread([&cs, dev] {
+    cs.rc = ag_ctx_create(dev, &cs.ctx);
+    if (cs.rc != AG_OK) cs.err = ag_last_error();
+  });
   Timer t0;
   ag::loadGPF(p, lib, log, gpf.empty() ? nullptr : gpf.c_str());
   const double parseMs = t0.ms();
@@ -1479,10 +1501,15 @@ int runMain(int argc, char** argv) {
     fprintf(stderr, "Writing .fld             Real: %.1f ms\n", fldMs);
   }
 
-  Timer tc;
-  ag_ctx* ctx = nullptr;
-  if (ag_ctx_create(dev, &ctx) != AG_OK) log.fatal(-2, "%s", ag_last_error());
-  if (bench) fprintf(stderr, "CUDA context             Real: %.1f ms\n", tc.ms());
+  Timer tw;
+  cs.th.join();
+  if (cs.rc != AG_OK) log.fatal(-2, "%s", cs.err.c_str());
+  ag_ctx* ctx = cs.ctx;
+  cs.ctx = nullptr;
+  if (bench) {
+    fprintf(stderr, "CUDA context             Real: %.1f ms\n", tc.ms());
+    fprintf(stderr, "  (waited after the host steps: %.1f ms)\n", tw.ms());
+  }
   ag_problem P;
   P.p = std::move(p);
   for (auto& m : P.p.maps) {
