@@ -116,9 +116,17 @@ __device__ __forceinline__ void run_type(const Aff2Params& P, const A2Smem& S, c
   const float4* tab4 = reinterpret_cast<const float4*>(tab);
   const int rowQ = nmPad >> 2;       // float4 per row
 
+  // The next candidate's record is read one iteration ahead (its shared-memory
+  // latency overlaps the current candidate's arithmetic).
+  int cNext = j0 < j1 ? wl[j0] : 0;
+  float4 aNext = j0 < j1 ? S.pos[cNext] : make_float4(0.f, 0.f, 0.f, 0.f);
   for (int jj = j0; jj < j1; jj++) {
-    const int c = wl[jj];
-    const float4 a = S.pos[c];
+    const int c = cNext;
+    const float4 a = aNext;
+    if (jj + 1 < j1) {
+      cNext = wl[jj + 1];
+      aNext = S.pos[cNext];
+    }
     const float dx = a.x - q.px, dy = a.y - q.py;
     const float dxy = fmaf(dy, dy, dx * dx);
     float dz[2], r2[2];
