@@ -100,9 +100,10 @@ struct ag_ctx {
   int emapMode = agk::kEmapKahan;
   float rNear = 11.0f;
   float delta = 2.0e-3f;
-  int anaPairs = 0;  // of each thread's 4 point pairs, those evaluating mid atoms' dielectric analytically
-                     // (none: measured fastest on B200, the analytic pairs' ex2 and series cost more than the
-                     // table reads they replace)
+  int packedTable = 1;              // AG_TUNE_EMAP_PACKED_TABLE
+  agc::DevBuf<uint4> epsPacked;     // 16- and 8-bit copies of the staged table's saturating tail
+  int pkVecs = 0, pkVec8 = 0, pkB16 = 8192, pkB8 = 8192;  // pkVecs == 0: no packed table
+  float pkScale = 0;
   int ctasPerSm = agk::kEmapCtasPerSm;
   agc::DevBuf<double> checksum;
   int checksumSplits = 0;

@@ -11,6 +11,7 @@ constexpr int kEmapKahan = 0;
 constexpr int kEmapPlain = 1;
 constexpr int kItemInterleaved = 1 << 30;  // e-map item flag: x points shared alternately with the partner column
 constexpr int kEmapCtasPerSm = 3;  // e-map CTAs resident per SM (register bound 85)
+constexpr int kEmapPackedBytes = 16384;  // e-map: shared-memory region of the packed table tail
 
 // A CTA's work in the e-map: items [item0, item0+nitems) of the item list and
 // the CTA's box: local origin (grid-centred frame, A) and half extents
@@ -36,10 +37,16 @@ struct EmapParams {
   const double* thr;              // thr[k]: least r^2 whose reference bin is >= k
   float rnear2;                   // (100 * rNear)^2
   float delta;                    // guard half-width around bin edges (units of 0.01 A)
-  int anaPairs;                   // of a thread's kNX/2 point pairs, how many evaluate mid atoms' bins analytically
-  float2 negBias2;                // -2^23, both halves: bin = f + negBias2
-  float2 negLambda2;              // -0.3153767175 / 100 / ln 2, both halves: E = 2^(negLambda2 * bin)
-  float2 poly2[6];                // invEps(bin) = sum_n poly2[n] E^n (both halves equal) for E <= 0.031
+  // Packed copies of the table's saturating tail (null: not used).  Entry b
+  // of the table, for b >= b16 (b8), is bits(table[8191]) + k with k stored
+  // in 16 (8) bits; the 16-bit entries for bins [b16, 8192) come first, then
+  // the 8-bit entries for bins [b8, 8192), each part padded to 16 bytes.
+  const uint4* packed;
+  int packedVecs;                 // 16-byte vectors in `packed`
+  int vec8;                       // vector at which the 8-bit part starts
+  int b16, b8;
+  float r16sq, r8sq;              // (b16 + 2)^2, (b8 + 2)^2: mid atoms at least that far (0.01 A units) from the box
+  float kScale;                   // 2^(e + 126) / g, g = table[8191] = 2^e * m: turns 100 w g 2^-16 into 100 w ulp(g) 2^133
   int testIdleWait;               // test hook: > 0 adds a wait of that many polls on a barrier nothing arrives on
   float* out;
   double* partial;                // nsplit * npoints, when nsplit > 1

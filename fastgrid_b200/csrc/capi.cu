@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -170,9 +171,9 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
       if (!(v >= 8.0 && v <= 40.0)) return fail(AG_E_INVALID, "rNear must be in [8, 40] A");
       c->rNear = (float)v;
       return AG_OK;
-    case AG_TUNE_EMAP_ANALYTIC_PAIRS:
-      if (!(v == 0.0 || v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "analytic point pairs must be 0, 1 or 2");
-      c->anaPairs = (int)v;
+    case AG_TUNE_EMAP_PACKED_TABLE:
+      if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "packed-table switch must be 0 or 1");
+      c->packedTable = (int)v;
       return AG_OK;
     case AG_TUNE_EMAP_WARP_COMPACT:
       if (!(v == 0.0 || v == 1.0 || v == 2.0)) return fail(AG_E_INVALID, "e-map item order must be 0, 1 or 2");
@@ -325,6 +326,62 @@ void buildItems(ag_ctx* c) {
   c->itemsTile = c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2];
 }
 
+// 16- and 8-bit copies of the FP32 table's saturating tail.  With g = t[8191]
+// and G = bits(g), entry b is G + k_b, k_b < 2^16 (2^8), for every bin from
+// b16 (b8) on, all of them in g's binade, so that k_b counts units in the last
+// place of g and g + k_b ulp(g) = t[b] exactly.  The two parts are padded to
+// 16 bytes and must fit the kernel's 16 KB region; b16 moves up until they do.
+// Returns the vectors (empty: no usable tail).
+std::vector<uint4> packTableTail(const std::vector<float>& t, int& b16, int& b8, int& vec8, float& kScale) {
+  const int n = (int)t.size();
+  std::vector<uint4> out;
+  b16 = b8 = n;
+  vec8 = 0;
+  kScale = 0.f;
+  const float g = t[n - 1];
+  if (!(std::isfinite(g) && g >= FLT_MIN)) return out;
+  uint32_t G;
+  std::memcpy(&G, &g, 4);
+  const uint32_t expG = G >> 23;
+  auto first = [&](uint32_t kmax) {
+    int b = n;
+    while (b > 0) {
+      uint32_t u;
+      std::memcpy(&u, &t[b - 1], 4);
+      if ((u >> 31) || (u >> 23) != expG || u < G || u - G > kmax) break;
+      b--;
+    }
+    return b;
+  };
+  b16 = first(0xFFFFu);
+  b8 = first(0xFFu);
+  auto bytes = [&](int b16_) { return ((2 * (n - b16_) + 15) / 16) * 16 + ((n - b8 + 15) / 16) * 16; };
+  while (b16 < n && bytes(b16) > agk::kEmapPackedBytes) b16 += 8;
+  if (b16 >= n) {
+    b16 = b8 = n;
+    return out;
+  }
+  const int v16 = (2 * (n - b16) + 15) / 16;
+  vec8 = v16;
+  std::vector<unsigned char> raw((size_t)bytes(b16), 0);
+  for (int b = b16; b < n; b++) {
+    uint32_t u;
+    std::memcpy(&u, &t[b], 4);
+    const uint16_t k = (uint16_t)(u - G);
+    std::memcpy(&raw[2 * (size_t)(b - b16)], &k, 2);
+  }
+  for (int b = b8; b < n; b++) {
+    uint32_t u;
+    std::memcpy(&u, &t[b], 4);
+    raw[16 * (size_t)v16 + (b - b8)] = (unsigned char)(u - G);
+  }
+  out.resize(raw.size() / 16);
+  std::memcpy(out.data(), raw.data(), raw.size());
+  // 2^(e + 126) / g with g = 2^e m, 1 <= m < 2.
+  kScale = (float)(std::ldexp(1.0, (int)expG - 127 + 126) / (double)g);
+  return out;
+}
+
 int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const double* inv_eps, bool deviceInputs) {
   if (int r = checkGrid(g)) return r;
   if (n < 0 || (n > 0 && !xyzw)) return fail(AG_E_INVALID, "bad atom array");
@@ -353,6 +410,12 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
     for (int i = 0; i < 8192; i++) t[i] = (float)inv_eps[i];
     CK(c->epsTab.ensure(8192));
     CK(cudaMemcpyAsync(c->epsTab.p, t.data(), sizeof(float) * 8192, cudaMemcpyHostToDevice, c->stream));
+    const std::vector<uint4> pk = packTableTail(t, c->pkB16, c->pkB8, c->pkVec8, c->pkScale);
+    c->pkVecs = (int)pk.size();
+    if (!pk.empty()) {
+      CK(c->epsPacked.ensure(pk.size()));
+      CK(cudaMemcpyAsync(c->epsPacked.p, pk.data(), sizeof(uint4) * pk.size(), cudaMemcpyHostToDevice, c->stream));
+    }
     CK(cudaStreamSynchronize(c->stream));
   }
   buildItems(c);
@@ -383,22 +446,15 @@ int buildEmapParams(ag_ctx* c, float* dOut, bool allowSplit, agk::EmapParams& P)
   P.thr = c->thr.p;
   P.rnear2 = (100.f * c->rNear) * (100.f * c->rNear);
   P.delta = c->delta;
-  // Series of 332/eps in E = exp(-0.3153767175 r): 332 (1 + a E) / (78.4 - c E)
-  // = (332 / 78.4) (1 + a E) sum_n (c / 78.4)^n E^n.
-  {
-    const double a = 7.7839, rho = 66.57180475 / 78.4, g0 = 332.0 / 78.4;
-    double rp = 1.0;
-    P.poly2[0] = make_float2((float)g0, (float)g0);
-    for (int n = 1; n < 6; n++) {
-      const double prev = rp;
-      rp *= rho;
-      const float v = (float)(g0 * (rp + a * prev));
-      P.poly2[n] = make_float2(v, v);
-    }
-    const float nl = (float)(-0.3153767175 / 100.0 / std::log(2.0));
-    P.negLambda2 = make_float2(nl, nl);
-    P.negBias2 = make_float2(-8388608.f, -8388608.f);
-    P.anaPairs = c->anaPairs;
+  if (c->ddd && c->packedTable && c->pkVecs > 0) {
+    P.packed = c->epsPacked.p;
+    P.packedVecs = c->pkVecs;
+    P.vec8 = c->pkVec8;
+    P.b16 = c->pkB16;
+    P.b8 = c->pkB8;
+    P.r16sq = (float)((c->pkB16 + 2.0) * (c->pkB16 + 2.0));
+    P.r8sq = (float)((c->pkB8 + 2.0) * (c->pkB8 + 2.0));
+    P.kScale = c->pkScale;
   }
   P.out = dOut;
   P.status = c->status.p;

@@ -23,6 +23,16 @@
 //      far (d >= rFar, at least 50 A): the table has saturated there (its
 //        entries differ from entry 8191 by < 2e-6 relative), so the term is
 //        w * invEps[8191] / r with no table read.
+//    Mid atoms whose every bin lies in the table's saturating tail read a
+//    packed copy of it instead: entry b is bits(g) + k_b, g = invEps[8191],
+//    with k_b < 2^16 from about 22 A and < 2^8 from about 40 A.  Half- and
+//    quarter-width entries put two or four neighbouring bins in one 32-bit
+//    shared-memory word, so a warp's reads (its lanes' distances span ~1 A,
+//    ~100 bins) touch fewer distinct words per bank: 2.0 and 1.5 wavefronts
+//    per read instead of 2.6 (simulated), and those wavefronts are the
+//    kernel's binding resource.  Decoding costs no instruction: k_b read as
+//    float bits is the subnormal k_b 2^-149, and one packed FMA forms
+//    100 w 2^-16 (g + k_b ulp(g)) = 100 w 2^-16 invEps[b] from it.
 //    Mid and far terms are summed in plain FP32 over chunks of kChunk atoms
 //    and the chunk sums are Kahan-compensated.
 //  * When the grid is too small to fill the GPU, atoms are split across CTAs
@@ -44,14 +54,18 @@ constexpr int kTile = 256;        // atoms per shared-memory tile
 constexpr int kTabLen = 8192;     // invEps entries
 constexpr int kChunk = 32;        // atoms per plain-FP32 chunk sum
 
+// Atom classes of a tile, in their order in EmapSmem::list.
+enum { kClsNear = 0, kClsMid = 1, kClsMid16 = 2, kClsMid8 = 3, kClsFar = 4, kNumCls = 5 };
+
 struct EmapSmem {
   float tab[kTabLen];             // 32 KB
   double4 ring[2][kTile];         // 16 KB, TMA destination
-  float4 nearA[kTile];            // local scaled x, y, z and 100*w
-  float4 midA[kTile];             // mid atoms, table read
-  float4 farA[kTile];             // w pre-multiplied by invEps[8191]
+  __align__(16) unsigned char packed[kEmapPackedBytes];
+  // This tile's atoms grouped by class: local scaled x, y, z and 100*w
+  // (near, mid), 100*w*g*2^-16 (packed mid) or 100*w*g (far).
+  float4 list[kTile];
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
-  int cnt[3][kThreads / 32];
+  int cnt[kNumCls][kThreads / 32];
   double wpart[kThreads / 32];
   int unit;                       // persistent batch kernel: the unit being processed
   uint64_t bar[2];
@@ -109,29 +123,13 @@ __device__ __forceinline__ float lds_bin(uint32_t tabBiased, float f) {
   return v;
 }
 
-__device__ __forceinline__ float ex2_approx(float x) {
-  float y;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// Mid-list atoms: bin by a round-down FMA, plain FP32 chunk sums.
-// The bin's value is read from the shared-memory table for the first
-// kNX/2 - NA point pairs of the thread and evaluated on the FMA and SFU pipes
-// for the last NA pairs:
-//   invEps(bin) = 332 (1 + a E) / (78.4 - c E),  E = exp(-0.3153767175 bin / 100)
-//   (autogrid.h:233-239), as the series sum_n P.poly2[n] E^n; mid atoms are
-//   at least rNear (default 11 A) away, so E <= 0.031 and the truncation is
-//   below 1e-8 relative (1e-6 at the smallest allowed rNear, 8 A).
-// The table reads' bank conflicts make shared-memory wavefronts the kernel's
-// limit; evaluating some pairs analytically in the same instruction stream
-// moves that work onto the SFU (ex2) and FMA pipes, which run in parallel.
+// Mid-list atoms: bin by a round-down FMA, table read, plain FP32 chunk sums.
 // CLAMP: the CTA's box is large enough that a bin can pass the table's end.
 // gxn holds minus the thread's x coordinates, in pairs (x0, x1), (x2, x3), ...
-template <int MODE, bool CLAMP, int NA>
+template <int MODE, bool CLAMP>
 __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint32_t tabBiased, int n,
                                           const float2 (&gxn)[kNX / 2], float gy, float gz, float2 (&sum)[kNX / 2],
-                                          float2 (&cmp)[kNX / 2], const EmapParams& P) {
+                                          float2 (&cmp)[kNX / 2]) {
   const float kBias = 8388608.f;
   const float2 bias2 = dup2(kBias);
 #pragma unroll 1
@@ -159,18 +157,7 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
           f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
           f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
         }
-        float2 g;
-        if (k >= kNX / 2 - NA) {
-          const float2 arg = __fmul2_rn(__fadd2_rn(f, P.negBias2), P.negLambda2);
-          const float2 E = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
-          g = __ffma2_rn(E, P.poly2[5], P.poly2[4]);
-          g = __ffma2_rn(E, g, P.poly2[3]);
-          g = __ffma2_rn(E, g, P.poly2[2]);
-          g = __ffma2_rn(E, g, P.poly2[1]);
-          g = __ffma2_rn(E, g, P.poly2[0]);
-        } else {
-          g = make_float2(lds_bin(tabBiased, f.x), lds_bin(tabBiased, f.y));
-        }
+        const float2 g = make_float2(lds_bin(tabBiased, f.x), lds_bin(tabBiased, f.y));
         cs[k] = __ffma2_rn(__fmul2_rn(aw, rs), g, cs[k]);
       }
     }
@@ -178,16 +165,58 @@ __device__ __forceinline__ void mid_atoms(const float4* __restrict__ list, uint3
   }
 }
 
-template <int MODE, bool CLAMP>
-__device__ __forceinline__ void mid_atoms_any(const float4* __restrict__ list, uint32_t tabBiased, int n,
-                                              const float2 (&gxn)[kNX / 2], float gy, float gz, float2 (&sum)[kNX / 2],
-                                              float2 (&cmp)[kNX / 2], const EmapParams& P) {
-  if (P.anaPairs == 1)
-    mid_atoms<MODE, CLAMP, 1>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
-  else if (P.anaPairs == 2)
-    mid_atoms<MODE, CLAMP, 2>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
+// Entry k_b of a packed tail table (W = 2: 16-bit, W = 1: 8-bit) at the bin
+// encoded in f = 2^23 + bin, returned as float bits (the subnormal k_b 2^-149).
+// tabBiased = address(entry 0) - W * (bits(2^23) + first bin), mod 2^32.
+template <int W>
+__device__ __forceinline__ float lds_packed(uint32_t tabBiased, float f) {
+  uint32_t v;
+  if (W == 2)
+    asm("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(tabBiased + ((uint32_t)__float_as_int(f) << 1)));
   else
-    mid_atoms<MODE, CLAMP, 0>(list, tabBiased, n, gxn, gy, gz, sum, cmp, P);
+    asm("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(tabBiased + (uint32_t)__float_as_int(f)));
+  return __uint_as_float(v);
+}
+
+// Mid atoms whose bins all lie in a packed tail table.  With a.w = 100 w g
+// 2^-16 and kScale = 2^(e+126) / g (g = 2^e m), aws = a.w kScale = 100 w
+// ulp(g) 2^133, so aws * k_b 2^-149 + a.w = 100 w 2^-16 (g + k_b ulp(g)):
+// the term's weight times the table entry, scaled by 2^-16 (exact), in one
+// FMA whose product is exact for 8-bit k_b and rounded once for 16-bit.  The
+// chunk sums run in the same scale and are scaled back by 2^16 (exact).
+template <int MODE, int W>
+__device__ __forceinline__ void mid_packed_atoms(const float4* __restrict__ list, uint32_t tabBiased, int n,
+                                                 const float2 (&gxn)[kNX / 2], float gy, float gz,
+                                                 float2 (&sum)[kNX / 2], float2 (&cmp)[kNX / 2], float kScale) {
+  const float2 bias2 = dup2(8388608.f);
+  const float2 down = dup2(1.0f / 65536.f), up = dup2(65536.f);
+#pragma unroll 1
+  for (int j0 = 0; j0 < n; j0 += kChunk) {
+    float2 cs[kNX / 2];
+#pragma unroll
+    for (int k = 0; k < kNX / 2; k++)
+      cs[k] = (MODE == kEmapKahan) ? make_float2(0.f, 0.f) : __fmul2_rn(sum[k], down);
+    const int j1 = min(n, j0 + kChunk);
+#pragma unroll 8
+    for (int j = j0; j < j1; j++) {
+      const float4 a = list[j];
+      const float dy = a.y - gy, dz = a.z - gz;
+      const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy));
+      const float2 ax = dup2(a.x), awg = dup2(a.w), aws = dup2(a.w * kScale);
+#pragma unroll
+      for (int k = 0; k < kNX / 2; k++) {
+        const float2 dx = __fadd2_rn(ax, gxn[k]);
+        const float2 r2 = __ffma2_rn(dx, dx, dyz2);
+        const float2 rs = rsqrt2(r2);
+        const float2 f = __ffma2_rd(r2, rs, bias2);
+        const float2 kb = make_float2(lds_packed<W>(tabBiased, f.x), lds_packed<W>(tabBiased, f.y));
+        cs[k] = __ffma2_rn(rs, __ffma2_rn(aws, kb, awg), cs[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kNX / 2; k++) cs[k] = __fmul2_rn(cs[k], up);
+    add_chunk<MODE>(sum, cmp, cs);
+  }
 }
 
 // One work unit: CTA box `blk` of job P against atom split `split`.  Called
@@ -221,10 +250,16 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
 #pragma unroll
   for (int k = 0; k < kNX / 2; k++) gxn[k] = make_float2(-gx[2 * k], -gx[2 * k + 1]);
 
+  // Packed tail tables for this box: only when no bin can pass the table's end.
+  const bool pk = DDD && P.packed != nullptr && !B.clampMid;
   if (DDD) {
     const float4* src = reinterpret_cast<const float4*>(P.table);
     float4* dst = reinterpret_cast<float4*>(S.tab);
     for (int i = tid; i < kTabLen / 4; i += kThreads) dst[i] = src[i];
+    if (pk) {
+      uint4* pdst = reinterpret_cast<uint4*>(S.packed);
+      for (int i = tid; i < P.packedVecs; i += kThreads) pdst[i] = P.packed[i];
+    }
   }
   if (tid == 0) {
     mbar_init(&S.bar[0], 1);
@@ -275,7 +310,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     }
 
     // Classify and convert this tile's atoms (one atom per thread).
-    int cls = -1;  // 0 near, 1 mid, 2 far
+    int cls = -1;
     float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < nt) {
       double4 a = S.ring[slot][tid];
@@ -287,48 +322,71 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       const float dx = fmaxf(fabsf(loc.x) - B.hx, 0.f), dy = fmaxf(fabsf(loc.y) - B.hy, 0.f),
                   dz = fmaxf(fabsf(loc.z) - B.hz, 0.f);
       const float d2 = dx * dx + dy * dy + dz * dz;
-      cls = d2 < P.rnear2 ? 0 : ((DDD && d2 < B.rfar2) ? 1 : 2);
-      if (cls == 2) loc.w *= gFar;
-    }
-    const unsigned b0 = __ballot_sync(0xffffffffu, cls == 0);
-    const unsigned b1 = __ballot_sync(0xffffffffu, cls == 1);
-    const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-    if (lane == 0) {
-      S.cnt[0][warp] = __popc(b0);
-      S.cnt[1][warp] = __popc(b1);
-      S.cnt[2][warp] = __popc(b2);
-    }
-    __syncthreads();
-    int nNear = 0, nMid = 0, nFar = 0, off0 = 0, off1 = 0, off2 = 0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; w++) {
-      if (w == warp) { off0 = nNear; off1 = nMid; off2 = nFar; }
-      nNear += S.cnt[0][w];
-      nMid += S.cnt[1][w];
-      nFar += S.cnt[2][w];
+      if (d2 < P.rnear2) {
+        cls = kClsNear;
+      } else if (DDD && d2 < B.rfar2) {
+        cls = kClsMid;
+        if (pk && d2 >= P.r16sq) {
+          cls = d2 >= P.r8sq ? kClsMid8 : kClsMid16;
+          loc.w *= gFar * (1.0f / 65536.f);
+        }
+      } else {
+        cls = kClsFar;
+        loc.w *= gFar;
+      }
     }
     const unsigned lt = (1u << lane) - 1u;
-    if (cls == 0) {
-      const int pos = off0 + __popc(b0 & lt);
-      S.nearA[pos] = loc;
-      S.nearIdx[pos] = (short)tid;
-    } else if (cls == 1) {
-      S.midA[off1 + __popc(b1 & lt)] = loc;
-    } else if (cls == 2) {
-      S.farA[off2 + __popc(b2 & lt)] = loc;
+    unsigned myBallot = 0;
+#pragma unroll
+    for (int c = 0; c < kNumCls; c++) {
+      const unsigned b = __ballot_sync(0xffffffffu, cls == c);
+      if (cls == c) myBallot = b;
+      if (lane == 0) S.cnt[c][warp] = __popc(b);
     }
     __syncthreads();
+    // Start of each class in the list, and of this warp's atoms within it.
+    int base[kNumCls];
+    int run = 0, myPos = 0;
+#pragma unroll
+    for (int c = 0; c < kNumCls; c++) {
+      base[c] = run;
+      int off = 0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; w++) {
+        const int v = S.cnt[c][w];
+        off += (w < warp) ? v : 0;
+        run += v;
+      }
+      if (cls == c) myPos = base[c] + off + __popc(myBallot & lt);
+    }
+    if (cls >= 0) {
+      S.list[myPos] = loc;
+      if (cls == kClsNear) S.nearIdx[myPos] = (short)tid;
+    }
+    __syncthreads();
+    const int nNear = base[kClsMid];
 
-    // Mid atoms: table read or analytic bin value.
+    // Mid atoms: table read, or a packed tail table.
     if (DDD) {
       const uint32_t tabBiased = smem_u32(S.tab) - 0x2C000000u;
+      const int nMid = base[kClsMid16] - base[kClsMid];
       if (B.clampMid)
-        mid_atoms_any<MODE, true>(S.midA, tabBiased, nMid, gxn, gy, gz, sum, cmp, P);
+        mid_atoms<MODE, true>(S.list + base[kClsMid], tabBiased, nMid, gxn, gy, gz, sum, cmp);
       else
-        mid_atoms_any<MODE, false>(S.midA, tabBiased, nMid, gxn, gy, gz, sum, cmp, P);
+        mid_atoms<MODE, false>(S.list + base[kClsMid], tabBiased, nMid, gxn, gy, gz, sum, cmp);
+      if (pk) {
+        const uint32_t p16 = smem_u32(S.packed) - 2u * (0x4B000000u + (uint32_t)P.b16);
+        const uint32_t p8 = smem_u32(S.packed) + 16u * (uint32_t)P.vec8 - (0x4B000000u + (uint32_t)P.b8);
+        mid_packed_atoms<MODE, 2>(S.list + base[kClsMid16], p16, base[kClsMid8] - base[kClsMid16], gxn, gy, gz, sum,
+                                  cmp, P.kScale);
+        mid_packed_atoms<MODE, 1>(S.list + base[kClsMid8], p8, base[kClsFar] - base[kClsMid8], gxn, gy, gz, sum,
+                                  cmp, P.kScale);
+      }
     }
 
     // Far atoms: saturated dielectric (or the constant dielectric), no table.
+    const int nFar = run - base[kClsFar];
+    const float4* farA = S.list + base[kClsFar];
 #pragma unroll 1
     for (int j0 = 0; j0 < nFar; j0 += kChunk) {
       float2 cs[kNX / 2];
@@ -338,7 +396,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       const int j1 = min(nFar, j0 + kChunk);
 #pragma unroll 8
       for (int j = j0; j < j1; j++) {
-        const float4 a = S.farA[j];
+        const float4 a = farA[j];
         const float dy = a.y - gy, dz = a.z - gz;
         const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy));
         const float2 ax = dup2(a.x), aw = dup2(a.w);
@@ -354,7 +412,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     // Near atoms: clamp 1/r at 2 and decide bins near an edge exactly.
 #pragma unroll 1
     for (int j = 0; j < nNear; j++) {
-      const float4 a = S.nearA[j];
+      const float4 a = S.list[j];
       const float dy = a.y - gy, dz = a.z - gz;
       // The 1e-30 keeps r2 > 0 (an atom on a grid point) without a per-point max.
       const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy) + 1e-30f);

@@ -91,7 +91,7 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
  * --cuda-* switches played this role for its kernels).  Results stay within
  * the stated tolerances for every allowed value. */
 #define AG_TUNE_EMAP_RNEAR 1          /* A, >= 8: atoms nearer the CTA box take the exact-bin path (default 11) */
-#define AG_TUNE_EMAP_ANALYTIC_PAIRS 2 /* 0..2: of each thread's 4 point pairs, how many evaluate 332/eps analytically for atoms beyond rNear instead of reading the table (default 0) */
+#define AG_TUNE_EMAP_PACKED_TABLE 2   /* 0/1: mid atoms in the table's saturating tail (from about 22 A) read 16- and 8-bit copies of it (1, default) or the FP32 table (0) */
 #define AG_TUNE_EMAP_CTAS_PER_SM 3    /* 1..8: CTAs per SM the atom split aims for on small grids (default 3) */
 #define AG_TUNE_EMAP_WARP_COMPACT 4   /* e-map item order: 0 rows, 1 each warp's items form a compact box, 2 as 1 with
                                          neighbouring lanes sharing a 16-point x span alternately (default 2) */
@@ -222,14 +222,14 @@ int ag_main(int argc, char** argv);
  * floats, 4-byte aligned); misaligned pointers are rejected with
  * AG_E_INVALID before any CUDA call.  Work is issued on `stream` (a
  * cudaStream_t, NULL for the default stream) and the call is synchronous: it
- * returns when that work is done.  Scratch lives in fixed device arrays of
+ * returns when that work is done, so it cannot be recorded into a stream
+ * capture (a call on a capturing stream fails with AG_E_CUDA).  Scratch lives in fixed device arrays of
  * the library (about 21 MiB on each device that loads it, kept until exit):
  * grids above about 8.4 million points (1,048,576 rows of 8 points) are
  * rejected with AG_E_INVALID, also before any CUDA call.  All calls share
  * those arrays and they keep the last call's contents, so calls whose GPU
  * work overlaps race; serialise them.  The first call on a device (and the
- * first after its context is re-created) performs that device's set-up; make
- * it before any stream capture.  Like ag_emap it checks the net charge: the
+ * first after its context is re-created) also performs that device's set-up.  Like ag_emap it checks the net charge: the
  * kernel's FP64 sum of the weights it consumed must equal the input's, else
  * AG_E_DEVICE. */
 int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps, float* d_out,

@@ -139,13 +139,22 @@ def test_emap_edge_cases(ctx):
         assert np.abs(got - ref).max() <= E_TOL * max(1.0, np.abs(ref).max() * 1e-3)
 
 
-@pytest.mark.parametrize("order,tile,ana", [(0, 11616, 0), (1, 11616, 0), (2, 20816, 0), (2, 21608, 0),
-                                            (2, 40808, 0), (1, 20816, 1), (2, 20816, 2)])
-def test_emap_item_orders_tiles_and_analytic_pairs(order, tile, ana):
+# Plain FP32 summation (AG_EMAP_PLAIN) of a few thousand atoms: its rounding
+# error stays well inside this bound, and a wrongly scaled packed-table sum
+# (a factor 2^16) or a missing term would not.
+PLAIN_TOL = 5e-4
+
+
+@pytest.mark.parametrize("order,tile,packed", [(0, 11616, 1), (1, 11616, 1), (2, 20816, 1), (2, 21608, 1),
+                                               (2, 40808, 1), (1, 20816, 0), (2, 20816, 0)])
+@pytest.mark.parametrize("mode", [fg.AG_EMAP_KAHAN, fg.AG_EMAP_PLAIN])
+def test_emap_item_orders_tiles_and_packed_table(order, tile, packed, mode):
     """Every e-map item order (rows, warp-compact, x-interleaved lane pairs),
-    several CTA tiles and the analytic-dielectric pairs against the oracle, on
-    grids whose x extent leaves partial and unpaired 8-point columns, with
-    atoms in the near, mid and far (saturated dielectric) classes."""
+    several CTA tiles, and the FP32 table against its packed 16- and 8-bit
+    tail copies, against the oracle in both summation modes, on grids whose x
+    extent leaves partial and unpaired 8-point columns, with atoms in the
+    near, mid, packed-mid (22-55 A from a CTA box) and far (saturated
+    dielectric) classes."""
     rng = np.random.default_rng(7)
     eps = np.zeros(8192)
     oracle.lib().oracle_ddd_table(oracle._dp(eps))
@@ -153,18 +162,21 @@ def test_emap_item_orders_tiles_and_analytic_pairs(order, tile, ana):
     try:
         c.tune(fg.AG_TUNE_EMAP_WARP_COMPACT, order)
         c.tune(fg.AG_TUNE_EMAP_TILE, tile)
-        c.tune(fg.AG_TUNE_EMAP_ANALYTIC_PAIRS, ana)
+        c.tune(fg.AG_TUNE_EMAP_PACKED_TABLE, packed)
         inner = rng.normal(0, 9.0, (2500, 3))
+        shell = rng.normal(0, 1.0, (900, 3))
+        shell = shell / np.linalg.norm(shell, axis=1, keepdims=True) * rng.uniform(20, 62, (900, 1))
         outer = rng.normal(0, 1.0, (60, 3))
         outer = outer / np.linalg.norm(outer, axis=1, keepdims=True) * rng.uniform(55, 75, (60, 1))
-        pts = np.concatenate([inner, outer])
+        pts = np.concatenate([inner, shell, outer])
         xyzw = np.concatenate([pts, rng.normal(0, 0.05, (len(pts), 1))], axis=1)
         for (nx, ny, nz) in [(33, 45, 29), (45, 41, 37)]:
             g = fg.Grid(nx, ny, nz, 0.375)
-            got = c.emap(g, xyzw, eps)
+            got = c.emap(g, xyzw, eps, mode=mode)
             ref = oracle.emap(g, xyzw, eps)
-            assert np.abs(got - ref).max() <= E_TOL, (order, tile, ana, (nx, ny, nz), np.abs(got - ref).max())
-            if ana == 0:
+            tol = E_TOL if mode == fg.AG_EMAP_KAHAN else PLAIN_TOL
+            assert np.abs(got - ref).max() <= tol, (order, tile, packed, (nx, ny, nz), np.abs(got - ref).max())
+            if packed == 1 and mode == fg.AG_EMAP_KAHAN:
                 got = c.emap(g, xyzw, None)
                 ref = oracle.emap(g, xyzw, None)
                 assert np.abs(got - ref).max() <= E_TOL * max(1.0, np.abs(ref).max() * 1e-3)

@@ -222,3 +222,46 @@ def test_shipped_surrogate_weights_match_their_training_report():
     assert rep["receptors"] == 200 and rep["epochs"] == 10 and len(rep["loss_per_epoch"]) == 10
     assert rep["last_epoch_loss"] < 0.1 * rep["first_epoch_loss"]
     assert rep["command"].startswith("python -m fastgrid_b200.train_surrogate")
+
+
+def test_packed_table_tail_reconstructs_the_fp32_table():
+    """The e-map's packed copies of the table's saturating tail (capi.cu
+    packTableTail, emap.cu mid_packed_atoms), restated: from bin b16 (b8) on
+    every FP32 entry is bits(t[8191]) + k with k < 2^16 (2^8), all in
+    t[8191]'s binade, and the kernel's one FMA  aws * (k as the subnormal
+    k 2^-149) + awg,  awg = 100 w t[8191] 2^-16 and aws = awg * 2^(e+126) /
+    t[8191], gives 100 w t[b] 2^-16 to within one FP32 rounding."""
+    t = np.asarray(fg.ddd_table(), dtype=np.float64).astype(np.float32)
+    u = t.view(np.uint32)
+    G = int(u[-1])
+    e = G >> 23
+
+    def first(kmax):
+        b = t.size
+        while b > 0:
+            x = int(u[b - 1])
+            if (x >> 31) or (x >> 23) != e or x < G or x - G > kmax:
+                break
+            b -= 1
+        return b
+
+    b16, b8 = first(0xFFFF), first(0xFF)
+    # About 22 A and 40 A; both parts fit the kernel's 16 KB region.
+    assert 2200 <= b16 <= 2300 and 3950 <= b8 <= 4050
+    assert ((2 * (8192 - b16) + 15) // 16 + (8192 - b8 + 15) // 16) * 16 <= 16384
+    g = np.float32(t[-1])
+    k_scale = np.float32(np.ldexp(1.0, e - 127 + 126) / float(g))
+    assert np.isfinite(k_scale)
+    bins = np.arange(b16, 8192)
+    k = (u[bins].astype(np.int64) - G).astype(np.uint32)
+    assert np.array_equal(u[bins], (G + k).astype(np.uint32))
+    kf = k.view(np.float32).astype(np.float64)  # subnormals k 2^-149
+    assert np.array_equal(kf, k.astype(np.float64) * 2.0 ** -149)
+    for w in (0.001, -0.137, 0.5, 2.0, -1.9, 300.0):
+        lw = np.float32(np.float64(w) * 100.0)
+        awg = np.float32(lw * g * np.float32(2.0 ** -16))
+        aws = np.float32(awg * k_scale)
+        assert np.isfinite(aws)
+        got = (np.float64(aws) * kf + np.float64(awg)).astype(np.float32).astype(np.float64)
+        want = float(lw) * t[bins].astype(np.float64) * 2.0 ** -16
+        assert np.abs(got / want - 1.0).max() <= 2.0 ** -23
