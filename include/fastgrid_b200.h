@@ -223,13 +223,15 @@ int ag_main(int argc, char** argv);
  * AG_E_INVALID before any CUDA call.  Work is issued on `stream` (a
  * cudaStream_t, NULL for the default stream) and the call is synchronous: it
  * returns when that work is done, so it cannot be recorded into a stream
- * capture (a call on a capturing stream fails with AG_E_CUDA).  Scratch lives in fixed device arrays of
- * the library (about 21 MiB on each device that loads it, kept until exit):
- * grids above about 8.4 million points (1,048,576 rows of 8 points) are
- * rejected with AG_E_INVALID, also before any CUDA call.  All calls share
- * those arrays and they keep the last call's contents, so calls whose GPU
- * work overlaps race; serialise them.  The first call on a device (and the
- * first after its context is re-created) also performs that device's set-up.  Like ag_emap it checks the net charge: the
+ * capture (a call on a capturing stream fails with AG_E_CUDA).  Scratch
+ * lives in fixed device arrays of the library (about 21 MiB on each device
+ * that loads it, kept until exit): grids above about 8.4 million points
+ * (1,048,576 rows of 8 points) are rejected with AG_E_INVALID, also before
+ * any CUDA call.  All calls share those arrays and they keep the last call's
+ * contents, so calls whose GPU work overlaps race; serialise them.  The first
+ * call on a device (and the first after its context is re-created) also
+ * performs that device's set-up.  The dielectric table is read in FP32 only
+ * (no packed tail copies).  Like ag_emap it checks the net charge: the
  * kernel's FP64 sum of the weights it consumed must equal the input's, else
  * AG_E_DEVICE. */
 int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps, float* d_out,
