@@ -326,20 +326,21 @@ void buildItems(ag_ctx* c) {
   c->itemsTile = c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2];
 }
 
-// 16- and 8-bit copies of the FP32 table's saturating tail.  With g = t[8191]
+// 16- and 8-bit copies of the FP32 table's saturating tail.  With g = t[n-1]
 // and G = bits(g), entry b is G + k_b, k_b < 2^16 (2^8), for every bin from
 // b16 (b8) on, all of them in g's binade, so that k_b counts units in the last
 // place of g and g + k_b ulp(g) = t[b] exactly.  The two parts are padded to
-// 16 bytes and must fit the kernel's 16 KB region; b16 moves up until they do.
-// Returns the vectors (empty: no usable tail).
-std::vector<uint4> packTableTail(const std::vector<float>& t, int& b16, int& b8, int& vec8, float& kScale) {
-  const int n = (int)t.size();
-  std::vector<uint4> out;
+// 16 bytes and must fit `cap` bytes; b16 moves up until they do.  Writes the
+// parts to raw and returns their size in bytes (0: no usable tail; b16 = b8
+// = n).  Allocates nothing.
+int packTableTailInto(const float* t, int n, unsigned char* raw, int cap, int& b16, int& b8, int& vec8,
+                      float& kScale) {
   b16 = b8 = n;
   vec8 = 0;
   kScale = 0.f;
+  if (n <= 0) return 0;
   const float g = t[n - 1];
-  if (!(std::isfinite(g) && g >= FLT_MIN)) return out;
+  if (!(std::isfinite(g) && g >= FLT_MIN)) return 0;
   uint32_t G;
   std::memcpy(&G, &g, 4);
   const uint32_t expG = G >> 23;
@@ -356,14 +357,15 @@ std::vector<uint4> packTableTail(const std::vector<float>& t, int& b16, int& b8,
   b16 = first(0xFFFFu);
   b8 = first(0xFFu);
   auto bytes = [&](int b16_) { return ((2 * (n - b16_) + 15) / 16) * 16 + ((n - b8 + 15) / 16) * 16; };
-  while (b16 < n && bytes(b16) > agk::kEmapPackedBytes) b16 += 8;
+  while (b16 < n && bytes(b16) > cap) b16 += 8;
   if (b16 >= n) {
     b16 = b8 = n;
-    return out;
+    return 0;
   }
   const int v16 = (2 * (n - b16) + 15) / 16;
   vec8 = v16;
-  std::vector<unsigned char> raw((size_t)bytes(b16), 0);
+  const int total = bytes(b16);
+  std::memset(raw, 0, (size_t)total);
   for (int b = b16; b < n; b++) {
     uint32_t u;
     std::memcpy(&u, &t[b], 4);
@@ -375,10 +377,17 @@ std::vector<uint4> packTableTail(const std::vector<float>& t, int& b16, int& b8,
     std::memcpy(&u, &t[b], 4);
     raw[16 * (size_t)v16 + (b - b8)] = (unsigned char)(u - G);
   }
-  out.resize(raw.size() / 16);
-  std::memcpy(out.data(), raw.data(), raw.size());
   // 2^(e + 126) / g with g = 2^e m, 1 <= m < 2.
   kScale = (float)(std::ldexp(1.0, (int)expG - 127 + 126) / (double)g);
+  return total;
+}
+
+// The same, into 16-byte vectors (empty: no usable tail).
+std::vector<uint4> packTableTail(const std::vector<float>& t, int& b16, int& b8, int& vec8, float& kScale) {
+  std::vector<uint4> out(agk::kEmapPackedBytes / 16);
+  const int bytes = packTableTailInto(t.data(), (int)t.size(), reinterpret_cast<unsigned char*>(out.data()),
+                                      agk::kEmapPackedBytes, b16, b8, vec8, kScale);
+  out.resize((size_t)bytes / 16);
   return out;
 }
 

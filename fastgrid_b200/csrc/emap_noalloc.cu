@@ -19,6 +19,10 @@
 // Sharing: every call, from any thread or stream, uses the same device arrays,
 // and they keep the previous call's contents.  Calls whose GPU work overlaps
 // race on them; serialise such calls (same stream, or wait between them).
+// The dielectric table is read back to the host on every call (32 KB) and its
+// saturating tail packed into 16- and 8-bit copies in a fixed device array, as
+// the ordinary entry points do.
+//
 // The per-device set-up (symbol addresses, the bin-threshold table) happens on
 // the first call on each device, and again on the first call after the
 // device's context was re-created (e.g. after cudaDeviceReset); make that
@@ -45,6 +49,8 @@ void setLastError(const char* msg);  // capi.cu
 }
 namespace agc {
 void emapBinThresholdsInto(double* thr);  // capi.cu: fills thr[0 .. 8192], no allocation
+int packTableTailInto(const float* t, int n, unsigned char* raw, int cap, int& b16, int& b8, int& vec8,
+                      float& kScale);  // capi.cu: packed tail tables of the dielectric table, no allocation
 }
 
 namespace {
@@ -62,6 +68,7 @@ static __device__ __align__(256) double g_naThr[kNaThr];
 static __device__ __align__(256) unsigned g_naStatus[64];
 static __device__ __align__(256) double g_naChecksum[kNaMaxSplit];
 static __device__ __align__(256) double g_naWeights[2];  // input sum w, sum |w|
+static __device__ __align__(256) uint4 g_naPacked[agk::kEmapPackedBytes / 16];  // packed table tail
 
 struct NaDevice {
   bool ready = false;
@@ -73,6 +80,7 @@ struct NaDevice {
   unsigned* status = nullptr;
   double* checksum = nullptr;
   double* weights = nullptr;
+  uint4* packed = nullptr;
 };
 
 constexpr int kNaMaxDevices = 64;
@@ -86,6 +94,8 @@ double g_hThr[kNaThr];
 bool g_thrReady = false;
 double g_hChecksum[kNaMaxSplit];
 double g_hWeights[2];
+float g_hTab[8192];
+alignas(16) unsigned char g_hPacked[agk::kEmapPackedBytes];
 
 int naFail(int code, const char* msg) {
   ag::setLastError(msg);  // read back with ag_last_error()
@@ -158,7 +168,8 @@ int naSetup(NaDevice& d) {
       cudaGetSymbolAddress((void**)&d.thr, g_naThr) != cudaSuccess ||
       cudaGetSymbolAddress((void**)&d.status, g_naStatus) != cudaSuccess ||
       cudaGetSymbolAddress((void**)&d.checksum, g_naChecksum) != cudaSuccess ||
-      cudaGetSymbolAddress((void**)&d.weights, g_naWeights) != cudaSuccess)
+      cudaGetSymbolAddress((void**)&d.weights, g_naWeights) != cudaSuccess ||
+      cudaGetSymbolAddress((void**)&d.packed, g_naPacked) != cudaSuccess)
     return naFail(AG_E_CUDA, "cudaGetSymbolAddress failed for the no-allocation scratch arrays");
   unsigned long long id = 0;
   if (!naContextId(id)) return naFail(AG_E_CUDA, "cannot identify the current CUDA context");
@@ -279,6 +290,19 @@ extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d
       cudaMemsetAsync(D.status, 0, sizeof(unsigned), st) != cudaSuccess ||
       cudaMemsetAsync(D.checksum, 0xFF, sizeof(double) * nsplit, st) != cudaSuccess)  // NaN until written
     return naFail(AG_E_CUDA, "cannot stage the work list");
+  // The dielectric table's packed tail: the caller's table is read back
+  // (32 KB) and packed on the host, as for the ordinary entry points.
+  int pkBytes = 0, b16 = 8192, b8 = 8192, vec8 = 0;
+  float kScale = 0.f;
+  if (d_inv_eps) {
+    if (cudaMemcpyAsync(g_hTab, d_inv_eps, sizeof g_hTab, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return naFail(AG_E_CUDA, "cannot read the dielectric table");
+    pkBytes = agc::packTableTailInto(g_hTab, 8192, g_hPacked, agk::kEmapPackedBytes, b16, b8, vec8, kScale);
+    if (pkBytes > 0 &&
+        cudaMemcpyAsync(D.packed, g_hPacked, (size_t)pkBytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      return naFail(AG_E_CUDA, "cannot stage the packed table");
+  }
   // The host staging arrays are reused by the next call: wait for the copies.
   if (cudaStreamSynchronize(st) != cudaSuccess) return naFail(AG_E_CUDA, "stream error");
 
@@ -293,6 +317,16 @@ extern "C" int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d
   P.npoints = np;
   P.h = grid->spacing;
   P.table = d_inv_eps;
+  if (pkBytes > 0) {
+    P.packed = D.packed;
+    P.packedVecs = pkBytes / 16;
+    P.vec8 = vec8;
+    P.b16 = b16;
+    P.b8 = b8;
+    P.r16sq = (float)((b16 + 2.0) * (b16 + 2.0));
+    P.r8sq = (float)((b8 + 2.0) * (b8 + 2.0));
+    P.kScale = kScale;
+  }
   P.thr = D.thr;
   P.rnear2 = (100.f * 14.0f) * (100.f * 14.0f);
   P.delta = 2.0e-3f;

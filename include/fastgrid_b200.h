@@ -230,8 +230,9 @@ int ag_main(int argc, char** argv);
  * any CUDA call.  All calls share those arrays and they keep the last call's
  * contents, so calls whose GPU work overlaps race; serialise them.  The first
  * call on a device (and the first after its context is re-created) also
- * performs that device's set-up.  The dielectric table is read in FP32 only
- * (no packed tail copies).  Like ag_emap it checks the net charge: the
+ * performs that device's set-up.  Each call reads the dielectric table back
+ * to the host (32 KB) to pack its saturating tail, as ag_emap does.  Like
+ * ag_emap it checks the net charge: the
  * kernel's FP64 sum of the weights it consumed must equal the input's, else
  * AG_E_DEVICE. */
 int ag_emap_noalloc(const ag_grid* grid, int n_atoms, const double* d_xyzw, const float* d_inv_eps, float* d_out,

@@ -184,6 +184,24 @@ def test_emap_item_orders_tiles_and_packed_table(order, tile, packed, mode):
         c.close()
 
 
+@pytest.mark.parametrize("spacing", [1.0, 1.5, 2.0])
+def test_emap_coarse_grids(spacing, ctx):
+    """Coarse grids, whose CTA boxes are large: from 1.5 A a full box's
+    diagonal is long enough that a mid atom's bin can pass the table's end
+    (the clamped mid-list path, FP32 table only), while the smaller boxes at
+    the grid's edges still read the packed tail tables; atoms spread over
+    +-90 A so every class occurs."""
+    rng = np.random.default_rng(11)
+    eps = np.zeros(8192)
+    oracle.lib().oracle_ddd_table(oracle._dp(eps))
+    g = fg.Grid(45, 37, 41, spacing)
+    pts = np.concatenate([rng.uniform(-35, 35, (2500, 3)), rng.uniform(-90, 90, (700, 3))])
+    xyzw = np.concatenate([pts, rng.normal(0, 0.1, (len(pts), 1))], axis=1)
+    got = ctx.emap(g, xyzw, eps)
+    ref = oracle.emap(g, xyzw, eps)
+    assert np.abs(got - ref).max() <= E_TOL, (spacing, np.abs(got - ref).max())
+
+
 def test_large_config_sampled(tmp_path, ctx):
     """The large benchmark configuration (20,000 atoms, 161^3, 10 ligand maps)
     against the oracle on 1500 sampled points."""
