@@ -124,7 +124,10 @@ extern "C" int ag_ctx_create(int device, ag_ctx** out) {
     delete c;
     return fail(AG_E_CUDA, "cudaStreamCreate failed");
   }
-  if (c->status.ensure(4) != cudaSuccess) {
+  // The status word must start at zero: cudaMalloc may hand back memory that
+  // a freed buffer of this process (another context's maps) left its values
+  // in, and kernels only ever set bits in it.
+  if (c->status.ensure(4) != cudaSuccess || cudaMemset(c->status.p, 0, sizeof(unsigned)) != cudaSuccess) {
     delete c;
     return fail(AG_E_NOMEM, "cannot allocate the status word");
   }

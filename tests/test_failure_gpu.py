@@ -63,3 +63,34 @@ def test_checksum_mismatch_is_reported(job):
         _ok(ctx, p, ref)
     finally:
         ctx.close()
+
+
+def test_fresh_context_ignores_stale_device_memory():
+    """A new context's status word starts clear even when the memory it gets
+    last held other data of this process: small device blocks are filled with
+    0xFF and freed (through the CUDA runtime), then contexts are created and
+    their first call is an e-map, which reads the status word back."""
+    from cuda.bindings import runtime as rt
+
+    rng = np.random.default_rng(3)
+    eps = np.zeros(8192)
+    oracle.lib().oracle_ddd_table(oracle._dp(eps))
+    g = fg.Grid(17, 13, 11, 0.375)
+    xyzw = np.concatenate([rng.uniform(-6, 6, (300, 3)), rng.normal(0, 0.1, (300, 1))], axis=1)
+    ref = oracle.emap(g, xyzw, eps)
+    for _ in range(4):
+        ptrs = []
+        for _ in range(16):
+            err, p = rt.cudaMalloc(64)
+            assert err == rt.cudaError_t.cudaSuccess
+            assert rt.cudaMemset(p, 0xFF, 64)[0] == rt.cudaError_t.cudaSuccess
+            ptrs.append(p)
+        assert rt.cudaDeviceSynchronize()[0] == rt.cudaError_t.cudaSuccess
+        for p in ptrs:
+            assert rt.cudaFree(p)[0] == rt.cudaError_t.cudaSuccess
+        ctx = fg.Context(0)
+        try:
+            got = ctx.emap(g, xyzw, eps)
+            assert np.abs(got.astype(np.float64) - ref).max() <= E_TOL
+        finally:
+            ctx.close()
