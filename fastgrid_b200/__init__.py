@@ -31,6 +31,7 @@ AG_EMAP_KAHAN, AG_EMAP_PLAIN = 0, 1
 AG_TUNE_EMAP_RNEAR, AG_TUNE_EMAP_PACKED_TABLE, AG_TUNE_EMAP_CTAS_PER_SM = 1, 2, 3
 AG_TUNE_EMAP_WARP_COMPACT, AG_TUNE_EMAP_TILE, AG_TUNE_SURROGATE_TCGEN05 = 4, 5, 6
 AG_TUNE_TEST_IDLE_WAIT, AG_TUNE_TEST_CHECKSUM_OFFSET, AG_TUNE_AFFINITY_KERNEL = 7, 8, 9
+AG_TUNE_CONCURRENT_PASSES = 10
 AG_E_INVALID, AG_E_CUDA, AG_E_DEVICE, AG_E_HOST, AG_E_NOMEM = -1, -2, -3, -4, -5
 TABLE_LEN = 8192
 

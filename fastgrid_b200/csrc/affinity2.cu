@@ -692,7 +692,7 @@ __device__ __forceinline__ void aff2_unit(const Aff2Params& P, const int cta, un
 template <int NMAX>
 __global__ void __launch_bounds__(kT, 2) affinity2_kernel(const __grid_constant__ Aff2Params P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  aff2_unit<NMAX>(P, blockIdx.x, smem_raw);
+  aff2_unit<NMAX>(P, P.ctaBase + blockIdx.x, smem_raw);
 }
 
 // Persistent kernel over the work units (job, CTA block) of a batch of
@@ -735,9 +735,15 @@ cudaError_t aff2_batch_launch(const Aff2Params* jobs, const int2* units, int nun
   return cudaGetLastError();
 }
 
-cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st) {
+cudaError_t aff2_launch_range(const Aff2Params& P0, int b0, int b1, cudaStream_t st) {
+  const int nb = ((P0.nx + 7) / 8) * ((P0.ny + 7) / 8) * ((P0.nz + 7) / 8);
+  b0 = max(0, b0);
+  b1 = min(nb, b1);
+  if (b1 <= b0) return cudaSuccess;
+  Aff2Params P = P0;
+  P.ctaBase = b0;
   const size_t smem = aff2_smem_bytes(P.nmPad);
-  const int grid = ((P.nx + 7) / 8) * ((P.ny + 7) / 8) * ((P.nz + 7) / 8);
+  const int grid = b1 - b0;
   cudaError_t e;
 #define AG_AFF2(N)                                                                                           \
   do {                                                                                                       \
@@ -752,5 +758,7 @@ cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st) {
 #undef AG_AFF2
   return cudaGetLastError();
 }
+
+cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st) { return aff2_launch_range(P, 0, 1 << 30, st); }
 
 }  // namespace agk

@@ -72,6 +72,7 @@ struct ag_ctx {
   int tile[3] = {2, 8, 16};   // e-map CTA tile in work items (x chunks of 8 points, y rows, z planes)
   int warpCompact = 2;        // e-map item order: 0 rows, 1 warp-compact, 2 warp-compact with x-interleaved lane pairs
   int itemsCompact = -1;      // the order hItems was built with
+  bool itemsOnDevice = false; // items / blocks hold hItems / hBlocks
   std::vector<double> epsHost;  // the staged 332/eps table (FP64), empty for the constant dielectric
   std::vector<double> atomsHost;  // host copy of the staged atoms (x, y, z, w)
   uint64_t atomsVersion = 0;      // bumped whenever new atoms are staged
@@ -117,6 +118,24 @@ struct ag_ctx {
     if (copyStream) return cudaSuccess;
     cudaError_t e = cudaStreamCreateWithFlags(&copyStream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evAff, cudaEventDisableTiming);
+    return e;
+  }
+  // Map set with both passes: the e-map on a high-priority stream and the
+  // affinity pass on `stream`, concurrently (AG_TUNE_CONCURRENT_PASSES).
+  int concurrentPasses = 1;
+  cudaStream_t emapStream = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  static constexpr int kMaxChunks = 8;  // z-slab chunks of the whole-job affinity pass
+  cudaEvent_t evChunk[kMaxChunks] = {};
+  cudaError_t ensureEmapStream() {
+    if (emapStream) return cudaSuccess;
+    int least = 0, greatest = 0;
+    cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&emapStream, cudaStreamNonBlocking, greatest);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming);
+    for (int k = 0; k < kMaxChunks && e == cudaSuccess; k++)
+      e = cudaEventCreateWithFlags(&evChunk[k], cudaEventDisableTiming);
     return e;
   }
   int64_t npoints() const { return (int64_t)grid.nx * grid.ny * grid.nz; }

@@ -196,9 +196,12 @@ struct Aff2Params {
   float* out;                     // this pass's first map: [nmaps][npoints]
   float* dmap;
   unsigned* status;
+  int ctaBase;                    // first CTA block of a launch (0, or a z-slab chunk's first block)
 };
 size_t aff2_smem_bytes(int nmPad);
 cudaError_t aff2_launch(const Aff2Params& P, cudaStream_t st);
+// Blocks [b0, b1) of the pass (the grid's CTA blocks run z-slab by z-slab).
+cudaError_t aff2_launch_range(const Aff2Params& P, int b0, int b1, cudaStream_t st);
 // CTA blocks (work units) of the two-point kernel on an nx x ny x nz grid.
 int aff2_ctas(int nx, int ny, int nz);
 // Persistent two-point pass over the units (job, CTA block) of many jobs.

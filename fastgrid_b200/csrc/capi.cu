@@ -163,6 +163,11 @@ extern "C" int ag_ctx_destroy(ag_ctx* c) {
   if (c->stream) cudaStreamDestroy(c->stream);
   if (c->copyStream) cudaStreamDestroy(c->copyStream);
   if (c->evAff) cudaEventDestroy(c->evAff);
+  if (c->emapStream) cudaStreamDestroy(c->emapStream);
+  if (c->evFork) cudaEventDestroy(c->evFork);
+  if (c->evJoin) cudaEventDestroy(c->evJoin);
+  for (cudaEvent_t ev : c->evChunk)
+    if (ev) cudaEventDestroy(ev);
   delete c;
   return AG_OK;
 }
@@ -206,6 +211,10 @@ extern "C" int ag_ctx_tune(ag_ctx* c, int knob, double v) {
     case AG_TUNE_TEST_CHECKSUM_OFFSET:
       if (!std::isfinite(v)) return fail(AG_E_INVALID, "checksum offset must be finite");
       c->testChecksumOffset = v;
+      return AG_OK;
+    case AG_TUNE_CONCURRENT_PASSES:
+      if (!(v == 0.0 || v == 1.0)) return fail(AG_E_INVALID, "concurrent-passes switch must be 0 or 1");
+      c->concurrentPasses = (int)v;
       return AG_OK;
     case AG_TUNE_EMAP_CTAS_PER_SM:
       if (!(v >= 1.0 && v <= 8.0)) return fail(AG_E_INVALID, "CTAs per SM must be 1..8");
@@ -321,6 +330,7 @@ void buildItems(ag_ctx* c) {
       c->itemsTile == c->tile[0] * 10000 + c->tile[1] * 100 + c->tile[2] && c->itemsCompact == c->warpCompact)
     return;
   makeItems(g, c->tile, c->warpCompact, c->hItems, c->hBlocks);
+  c->itemsOnDevice = false;
   c->itemsCompact = c->warpCompact;
   c->itemsFor[0] = g.nx;
   c->itemsFor[1] = g.ny;
@@ -431,12 +441,16 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
     CK(cudaStreamSynchronize(c->stream));
   }
   buildItems(c);
-  CK(c->items.ensure(c->hItems.size()));
-  CK(c->blocks.ensure(c->hBlocks.size()));
-  CK(cudaMemcpyAsync(c->items.p, c->hItems.data(), sizeof(int) * c->hItems.size(), cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(c->blocks.p, c->hBlocks.data(), sizeof(agk::EmapBlock) * c->hBlocks.size(),
-                     cudaMemcpyHostToDevice, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  if (!c->itemsOnDevice) {  // the work items and CTA boxes depend on the grid only
+    CK(c->items.ensure(c->hItems.size()));
+    CK(c->blocks.ensure(c->hBlocks.size()));
+    CK(cudaMemcpyAsync(c->items.p, c->hItems.data(), sizeof(int) * c->hItems.size(), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaMemcpyAsync(c->blocks.p, c->hBlocks.data(), sizeof(agk::EmapBlock) * c->hBlocks.size(),
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->itemsOnDevice = true;
+  }
   return AG_OK;
 }
 
@@ -859,6 +873,45 @@ int runAffinity(ag_ctx* c, float* dMaps, float* dDmap) {
   return AG_OK;
 }
 
+// The two-point affinity pass in z-slab chunks on the context's stream; as
+// each chunk finishes, the copy stream moves its rows of every affinity map
+// and of the d-map to `host` (page-locked, laid out [nMaps + 2][npoints] like
+// the device buffer).  Blocks run z-slab by z-slab, so a chunk of slabs is a
+// contiguous range of rows in every map.
+int runAffinityChunked(ag_ctx* c, float* host, int nchunks) {
+  const int64_t np = c->npoints();
+  const int nm = c->nMaps;
+  float* dMaps = c->maps.p;
+  float* dDmap = dMaps + (size_t)(nm + 1) * np;
+  if (int e = prepAffinity(c, c->stream)) return e;
+  std::vector<agk::Aff2Params> passes;
+  if (int e = buildAff2Params(c, dMaps, dDmap, passes)) return e;
+  const ag_grid& g = c->grid;
+  const int tbx = (g.nx + 7) / 8, tby = (g.ny + 7) / 8, slabs = (g.nz + 7) / 8;
+  const int64_t plane = (int64_t)g.nx * g.ny;
+  nchunks = std::max(1, std::min(nchunks, ag_ctx::kMaxChunks));
+  CK(c->ensureCopyStream());
+  CK(c->ensureEmapStream());
+  for (int k = 0; k < nchunks; k++) {
+    const int s0 = slabs * k / nchunks, s1 = slabs * (k + 1) / nchunks;
+    if (s1 <= s0) continue;
+    for (const auto& P : passes) {
+      CK(agk::aff2_launch_range(P, s0 * tbx * tby, s1 * tbx * tby, c->stream));
+      c->launches += 1;
+    }
+    CK(cudaEventRecord(c->evChunk[k], c->stream));
+    CK(cudaStreamWaitEvent(c->copyStream, c->evChunk[k], 0));
+    const int64_t z0 = 8LL * s0, z1 = std::min<int64_t>(8LL * s1, g.nz);
+    const size_t off = (size_t)(z0 * plane), cnt = (size_t)((z1 - z0) * plane);
+    for (int m = 0; m < nm; m++)
+      CK(cudaMemcpyAsync(host + (size_t)m * np + off, dMaps + (size_t)m * np + off, sizeof(float) * cnt,
+                         cudaMemcpyDeviceToHost, c->copyStream));
+    CK(cudaMemcpyAsync(host + (size_t)(nm + 1) * np + off, dDmap + off, sizeof(float) * cnt,
+                       cudaMemcpyDeviceToHost, c->copyStream));
+  }
+  return AG_OK;
+}
+
 int checkStatus(ag_ctx* c) {
   unsigned st = 0;
   CK(cudaMemcpyAsync(&st, c->status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
@@ -907,6 +960,24 @@ extern "C" int ag_compute(ag_ctx* c, int work) {
   CK(cudaSetDevice(c->device));
   const int64_t np = c->npoints();
   float* maps = c->maps.p;
+  if ((work & AG_WORK_EMAP) && (work & AG_WORK_AFFINITY) && c->haveAff && c->concurrentPasses) {
+    // Both passes at once: the e-map's CTAs go first on a high-priority
+    // stream and the affinity pass, on the context's stream, takes the SMs
+    // its last wave leaves free.  The outputs are disjoint; the context's
+    // stream waits for both.
+    CK(c->ensureEmapStream());
+    CK(cudaEventRecord(c->evFork, c->stream));
+    CK(cudaStreamWaitEvent(c->emapStream, c->evFork, 0));
+    std::swap(c->stream, c->emapStream);
+    int e = runEmap(c, maps + (size_t)c->nMaps * np);
+    std::swap(c->stream, c->emapStream);
+    if (e) return e;
+    CK(cudaEventRecord(c->evJoin, c->emapStream));
+    e = runAffinity(c, maps, maps + (size_t)(c->nMaps + 1) * np);
+    CK(cudaStreamWaitEvent(c->stream, c->evJoin, 0));
+    if (e) return e;
+    work &= ~(AG_WORK_EMAP | AG_WORK_AFFINITY);
+  }
   if (work & AG_WORK_EMAP)
     if (int e = runEmap(c, maps + (size_t)c->nMaps * np)) return e;
   if (work & AG_WORK_EMAP_SURROGATE)
@@ -1057,15 +1128,6 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
   if (int e = ag_upload(c, &g, &r, &a, eps)) return e;
   const int64_t np = c->npoints();
   const int nm = p.numMaps();
-  // Affinity, d-map and covalent maps first; their copy to the host then runs
-  // on a second stream while the e-map (most of the time) is computed.
-  if (int e = ag_compute(c, AG_WORK_AFFINITY)) return e;
-  for (int m = 0; m < nm; m++)
-    if (p.maps[m].isCovalent) {
-      CK(agk::covalent_launch(c->maps.p + (size_t)m * np, g.nx, g.ny, g.nz, g.spacing, p.covalentPoint,
-                              p.covHalfWidthSquaredInv, p.covBarrier, c->stream));
-      c->launches++;
-    }
   const size_t total = (size_t)(nm + 2) * np;
   if (P->pinnedN < total) {
     if (P->pinned) cudaFreeHost(P->pinned);
@@ -1074,15 +1136,48 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
     CK(cudaHostAlloc((void**)&P->pinned, sizeof(float) * total, cudaHostAllocDefault));
     P->pinnedN = total;
   }
+  bool anyCovalent = false;
+  for (int m = 0; m < nm; m++) anyCovalent |= p.maps[m].isCovalent;
   CK(c->ensureCopyStream());
-  CK(cudaEventRecord(c->evAff, c->stream));
-  CK(cudaStreamWaitEvent(c->copyStream, c->evAff, 0));
-  if (nm) CK(cudaMemcpyAsync(P->pinned, c->maps.p, sizeof(float) * nm * np, cudaMemcpyDeviceToHost, c->copyStream));
-  CK(cudaMemcpyAsync(P->pinned + (size_t)(nm + 1) * np, c->maps.p + (size_t)(nm + 1) * np, sizeof(float) * np,
-                     cudaMemcpyDeviceToHost, c->copyStream));
-  if (int e = ag_compute(c, AG_WORK_EMAP)) return e;
-  CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
-                     cudaMemcpyDeviceToHost, c->stream));
+  if (c->concurrentPasses && c->haveAff && useTwoPoint(c) && !anyCovalent) {
+    // Both passes at once (as ag_compute runs them): the e-map on the
+    // high-priority stream, its 17 MB copied back as soon as it is done; the
+    // affinity pass, which fills the SMs the e-map's last wave leaves free,
+    // in four z-slab chunks whose rows are copied back while later chunks
+    // run, so that little of the 184 MB of affinity maps is copied after the
+    // last kernel.
+    CK(c->ensureEmapStream());
+    CK(cudaEventRecord(c->evFork, c->stream));
+    CK(cudaStreamWaitEvent(c->emapStream, c->evFork, 0));
+    std::swap(c->stream, c->emapStream);
+    int e = ag_compute(c, AG_WORK_EMAP);
+    std::swap(c->stream, c->emapStream);
+    if (e) return e;
+    CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
+                       cudaMemcpyDeviceToHost, c->emapStream));
+    CK(cudaEventRecord(c->evJoin, c->emapStream));
+    e = runAffinityChunked(c, P->pinned, 4);
+    CK(cudaStreamWaitEvent(c->stream, c->evJoin, 0));
+    if (e) return e;
+  } else {
+    // Affinity, d-map and covalent maps first; their copy to the host then
+    // runs on a second stream while the e-map (most of the time) is computed.
+    if (int e = ag_compute(c, AG_WORK_AFFINITY)) return e;
+    for (int m = 0; m < nm; m++)
+      if (p.maps[m].isCovalent) {
+        CK(agk::covalent_launch(c->maps.p + (size_t)m * np, g.nx, g.ny, g.nz, g.spacing, p.covalentPoint,
+                                p.covHalfWidthSquaredInv, p.covBarrier, c->stream));
+        c->launches++;
+      }
+    CK(cudaEventRecord(c->evAff, c->stream));
+    CK(cudaStreamWaitEvent(c->copyStream, c->evAff, 0));
+    if (nm) CK(cudaMemcpyAsync(P->pinned, c->maps.p, sizeof(float) * nm * np, cudaMemcpyDeviceToHost, c->copyStream));
+    CK(cudaMemcpyAsync(P->pinned + (size_t)(nm + 1) * np, c->maps.p + (size_t)(nm + 1) * np, sizeof(float) * np,
+                       cudaMemcpyDeviceToHost, c->copyStream));
+    if (int e = ag_compute(c, AG_WORK_EMAP)) return e;
+    CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
+                       cudaMemcpyDeviceToHost, c->stream));
+  }
   CK(cudaStreamSynchronize(c->copyStream));
   if (int e = checkStatus(c)) return e;
   p.out.clear();
@@ -1143,6 +1238,7 @@ int restageItems(ag_ctx* c) {
   CK(c->blocks.ensure(c->hBlocks.size()));
   CK(cudaMemcpy(c->items.p, c->hItems.data(), sizeof(int) * c->hItems.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->blocks.p, c->hBlocks.data(), sizeof(agk::EmapBlock) * c->hBlocks.size(), cudaMemcpyHostToDevice));
+  c->itemsOnDevice = true;
   return AG_OK;
 }
 

@@ -101,6 +101,8 @@ int64_t ag_ctx_launch_count(const ag_ctx* ctx);
                                          nearest donor found in the kernel (default); 1 one point per thread
                                          with a separate nearest-donor kernel (also used for passes with more
                                          than 4 H-bond maps) */
+#define AG_TUNE_CONCURRENT_PASSES 10 /* 0/1: a map set's e-map and affinity pass run concurrently, the e-map on a
+                                         high-priority stream (1, default), or one after the other (0) */
 /* Failure-detection test hooks (default 0 = off).  IDLE_WAIT: 1..64 polls of an
  * extra wait, after each direct e-map CTA's first atom tile has landed, on a
  * barrier nothing arrives on; the wait expires, the kernel records it in its

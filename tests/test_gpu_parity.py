@@ -269,3 +269,32 @@ def test_cli_covalent_and_floating_grid(tmp_path):
     fld = open(os.path.join(work, "synth_covalent.maps.fld")).read().split("\n")
     ref = case["fld"].split("\n")
     assert [l for l in fld if not l.startswith("# Created by")] == [l for l in ref if not l.startswith("# Created by")]
+
+
+@pytest.mark.parametrize("kernel", [2, 1])
+def test_concurrent_passes_equal_sequential(tmp_path, kernel):
+    """The map set with the e-map and the affinity pass run concurrently (the
+    default; the whole-job call also copies the affinity maps back in z-slab
+    chunks) is bit-identical to the passes run one after the other, through
+    ag_compute and through the whole-job call, for both affinity kernels."""
+    fg.synth_write(str(tmp_path), "cc", n_atoms=2500, semi_axes=(16, 14, 12), npts=44, seed=23,
+                   ligand_types="A C HD N NA OA SA")
+    with chdir(str(tmp_path)):
+        p = fg.Problem("cc.gpf", log="cc.glg")
+    out = {}
+    for conc in (0, 1):
+        c = fg.Context(0)
+        try:
+            c.tune(fg.AG_TUNE_AFFINITY_KERNEL, kernel)
+            c.tune(fg.AG_TUNE_CONCURRENT_PASSES, conc)
+            c.upload(p.grid, p.receptor, p.params, p.inv_eps_ptr)
+            c.compute(fg.AG_WORK_ALL)
+            dev = np.empty((p.n_maps + 2) * p.npoints, dtype=np.float32)
+            c.download(dev)
+            p.compute(c)
+            out[conc] = (dev, p.maps().astype(np.float32).ravel().copy())
+        finally:
+            c.close()
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[1][0], out[1][1])
