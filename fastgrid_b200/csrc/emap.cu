@@ -65,6 +65,10 @@ struct EmapSmem {
   // (near, mid), 100*w*g*2^-16 (packed mid) or 100*w*g (far).
   float4 list[kTile];
   short nearIdx[kTile];           // tile slot of each near atom (for FP64 lookups)
+  // Near atom: bit w set if it lies within rNear of warp w's points, bit 8 + w
+  // if within 0.51 A of them (the 1/r cap can apply).
+  unsigned short nearMask[kTile];
+  float4 wlo[kThreads / 32], whi[kThreads / 32];  // each warp's box (local, scaled), widened by 0.01 A
   int cnt[kNumCls][kThreads / 32];
   double wpart[kThreads / 32];
   int unit;                       // persistent batch kernel: the unit being processed
@@ -219,6 +223,80 @@ __device__ __forceinline__ void mid_packed_atoms(const float4* __restrict__ list
   }
 }
 
+// One near atom against this thread's points, bins decided exactly near an
+// edge.  GUARD: cap 1/r at 2 and clamp the bin at the table's end; without it
+// the caller has shown that no point of the warp lies within 0.51 A of the
+// atom and that no bin can pass the table's end (the CTA box is small enough),
+// so neither would change a value.
+template <bool DDD, int MODE, bool GUARD>
+__device__ __forceinline__ void near_exact(const EmapSmem& S, const EmapParams& P, const int slot, const int j,
+                                           const float2 dyz2, const float2 ax, const float2 aw,
+                                           const float2 (&gxn)[kNX / 2], const int iy, const int iz, const int xb,
+                                           const int xs, float2 (&sum)[kNX / 2], float2 (&cmp)[kNX / 2]) {
+  const float cap = 0.02f;        // min(1/r, 2) in units of 1/(100 r)
+  const float kBias = 8388608.f;  // 2^23
+  const double h = P.h;
+  float2 rsv[kNX / 2];
+  float2 fT[kNX / 2];   // 100 r (FP32), kept for the rare exact-bin fallback
+  float2 fr5[kNX / 2];  // fraction of 100 r minus one half
+  uint32_t bits[kNX];   // 2^23 + bin, as float bits
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < kNX / 2; k++) {
+    const float2 dx = __fadd2_rn(ax, gxn[k]);
+    const float2 r2 = __ffma2_rn(dx, dx, dyz2);
+    rsv[k] = rsqrt2(r2);
+    if (DDD) {
+      fT[k] = __fmul2_rn(r2, rsv[k]);
+      float2 f = __ffma2_rd(r2, rsv[k], dup2(kBias));
+      if (GUARD) {
+        f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
+        f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
+      }
+      bits[2 * k] = __float_as_uint(f.x);
+      bits[2 * k + 1] = __float_as_uint(f.y);
+      // Within delta of a bin edge <=> the fraction of T is within delta of 0 or 1.
+      fr5[k] = __fadd2_rn(__fadd2_rn(fT[k], __ffma2_rn(f, dup2(-1.f), dup2(kBias))), dup2(-0.5f));
+      any |= (fabsf(fr5[k].x) > 0.5f - P.delta) | (fabsf(fr5[k].y) > 0.5f - P.delta);
+    }
+  }
+  if (DDD && __any_sync(0xffffffffu, any)) {
+    if (any) {
+      const double4 a64 = S.ring[slot][S.nearIdx[j]];
+      const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
+      const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
+      const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
+#pragma unroll
+      for (int k = 0; k < kNX; k++) {
+        if (fabsf(lo_hi(fr5[k >> 1], k)) > 0.5f - P.delta) {
+          // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
+          const int kmid = min(__float_as_int(lo_hi(fT[k >> 1], k) + 12582912.f) - 0x4B400000, kTabLen - 1);
+          const double gx64 = __dmul_rn((double)(xb + k * xs - P.n2x), h);
+          const double ddx = __dsub_rn(a64.x, gx64);
+          const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
+          const int b = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
+          bits[k] = 0x4B000000u + (uint32_t)b;
+        }
+      }
+    }
+  }
+  const uint32_t tabB = smem_u32(S.tab) - 0x2C000000u;  // address(tab) - 4 * bits(2^23)
+#pragma unroll
+  for (int k = 0; k < kNX / 2; k++) {
+    float2 term = __fmul2_rn(aw, GUARD ? make_float2(fminf(rsv[k].x, cap), fminf(rsv[k].y, cap)) : rsv[k]);
+    if (DDD) {
+      float2 t;
+      asm("ld.shared.f32 %0, [%1];" : "=f"(t.x) : "r"(tabB + (bits[2 * k] << 2)));
+      asm("ld.shared.f32 %0, [%1];" : "=f"(t.y) : "r"(tabB + (bits[2 * k + 1] << 2)));
+      term = __fmul2_rn(term, t);
+    }
+    if (MODE == kEmapKahan)
+      kahan2(sum[k], cmp[k], term);
+    else
+      sum[k] = __fadd2_rn(sum[k], term);
+  }
+}
+
 // One work unit: CTA box `blk` of job P against atom split `split`.  Called
 // once per CTA by emap_kernel, and repeatedly by the persistent batch kernel.
 template <bool DDD, int MODE>
@@ -259,6 +337,28 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     if (pk) {
       uint4* pdst = reinterpret_cast<uint4*>(S.packed);
       for (int i = tid; i < P.packedVecs; i += kThreads) pdst[i] = P.packed[i];
+    }
+  }
+  // This warp's box: the extent of its active lanes' points (an empty box,
+  // lo > hi, when no lane has an item), widened by 1 (0.01 A).
+  {
+    float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
+    if (active) {
+      lo[0] = fminf(gx[0], gx[kNX - 1]);
+      hi[0] = fmaxf(gx[0], gx[kNX - 1]);
+      lo[1] = hi[1] = gy;
+      lo[2] = hi[2] = gz;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+        hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+      }
+    if (lane == 0) {
+      S.wlo[warp] = make_float4(lo[0] - 1.f, lo[1] - 1.f, lo[2] - 1.f, 0.f);
+      S.whi[warp] = make_float4(hi[0] + 1.f, hi[1] + 1.f, hi[2] + 1.f, 0.f);
     }
   }
   if (tid == 0) {
@@ -311,6 +411,7 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
 
     // Classify and convert this tile's atoms (one atom per thread).
     int cls = -1;
+    unsigned nearBits = 0xFFFFu;
     float4 loc = make_float4(0.f, 0.f, 0.f, 0.f);
     if (tid < nt) {
       double4 a = S.ring[slot][tid];
@@ -324,6 +425,18 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       const float d2 = dx * dx + dy * dy + dz * dz;
       if (d2 < P.rnear2) {
         cls = kClsNear;
+        // The warps whose own points it is near: the others evaluate it as a mid atom.
+        unsigned m = 0;
+#pragma unroll
+        for (int w = 0; w < kThreads / 32; w++) {
+          const float4 wl = S.wlo[w], wh = S.whi[w];
+          const float ex = fmaxf(fmaxf(wl.x - loc.x, loc.x - wh.x), 0.f);
+          const float ey = fmaxf(fmaxf(wl.y - loc.y, loc.y - wh.y), 0.f);
+          const float ez = fmaxf(fmaxf(wl.z - loc.z, loc.z - wh.z), 0.f);
+          const float e2 = ex * ex + ey * ey + ez * ez;
+          m |= ((e2 < P.rnear2 ? 1u : 0u) << w) | ((e2 < 51.f * 51.f ? 1u : 0u) << (8 + w));
+        }
+        nearBits = m;
       } else if (DDD && d2 < B.rfar2) {
         cls = kClsMid;
         if (pk && d2 >= P.r16sq) {
@@ -361,7 +474,10 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
     }
     if (cls >= 0) {
       S.list[myPos] = loc;
-      if (cls == kClsNear) S.nearIdx[myPos] = (short)tid;
+      if (cls == kClsNear) {
+        S.nearIdx[myPos] = (short)tid;
+        S.nearMask[myPos] = (unsigned short)nearBits;
+      }
     }
     __syncthreads();
     const int nNear = base[kClsMid];
@@ -417,63 +533,33 @@ __device__ __forceinline__ void emap_unit(const EmapParams& P, const int blk, co
       // The 1e-30 keeps r2 > 0 (an atom on a grid point) without a per-point max.
       const float2 dyz2 = dup2(fmaf(dz, dz, dy * dy) + 1e-30f);
       const float2 ax = dup2(a.x), aw = dup2(a.w);
-      float2 rsv[kNX / 2];
-      float2 fT[kNX / 2];   // 100 r (FP32), kept for the rare exact-bin fallback
-      float2 fr5[kNX / 2];  // fraction of 100 r minus one half
-      uint32_t bits[kNX];   // 2^23 + bin, as float bits
-      bool any = false;
+      if (DDD && !((S.nearMask[j] >> warp) & 1u)) {
+        // At least rNear from every point of this warp (uniform): the mid-list
+        // arithmetic (no cap, round-down bin), each term compensated.  The
+        // clamp keeps the bin inside the table for any box size, and for the
+        // lanes without an item, whose stand-in points can lie anywhere.
+        const uint32_t tabB = smem_u32(S.tab) - 0x2C000000u;
 #pragma unroll
-      for (int k = 0; k < kNX / 2; k++) {
-        const float2 dx = __fadd2_rn(ax, gxn[k]);
-        const float2 r2 = __ffma2_rn(dx, dx, dyz2);
-        rsv[k] = rsqrt2(r2);
-        if (DDD) {
-          fT[k] = __fmul2_rn(r2, rsv[k]);
-          float2 f = __ffma2_rd(r2, rsv[k], dup2(kBias));
+        for (int k = 0; k < kNX / 2; k++) {
+          const float2 dx = __fadd2_rn(ax, gxn[k]);
+          const float2 r2 = __ffma2_rn(dx, dx, dyz2);
+          const float2 rs = rsqrt2(r2);
+          float2 f = __ffma2_rd(r2, rs, dup2(kBias));
           f.x = fminf(f.x, kBias + (float)(kTabLen - 1));
           f.y = fminf(f.y, kBias + (float)(kTabLen - 1));
-          bits[2 * k] = __float_as_uint(f.x);
-          bits[2 * k + 1] = __float_as_uint(f.y);
-          // Within delta of a bin edge <=> the fraction of T is within delta of 0 or 1.
-          fr5[k] = __fadd2_rn(__fadd2_rn(fT[k], __ffma2_rn(f, dup2(-1.f), dup2(kBias))), dup2(-0.5f));
-          any |= (fabsf(fr5[k].x) > 0.5f - P.delta) | (fabsf(fr5[k].y) > 0.5f - P.delta);
+          const float2 t = make_float2(lds_bin(tabB, f.x), lds_bin(tabB, f.y));
+          const float2 term = __fmul2_rn(__fmul2_rn(aw, rs), t);
+          if (MODE == kEmapKahan)
+            kahan2(sum[k], cmp[k], term);
+          else
+            sum[k] = __fadd2_rn(sum[k], term);
         }
+        continue;
       }
-      if (DDD && __any_sync(0xffffffffu, any)) {
-        if (any) {
-          const double4 a64 = S.ring[slot][S.nearIdx[j]];
-          const double gy64 = __dmul_rn((double)(iy - P.n2y), h), gz64 = __dmul_rn((double)(iz - P.n2z), h);
-          const double ddz = __dsub_rn(a64.z, gz64), ddy = __dsub_rn(a64.y, gy64);
-          const double dydz = __dadd_rn(__dmul_rn(ddy, ddy), __dmul_rn(ddz, ddz));
-#pragma unroll
-          for (int k = 0; k < kNX; k++) {
-            if (fabsf(lo_hi(fr5[k >> 1], k)) > 0.5f - P.delta) {
-              // The reference's bin is kmid - 1 or kmid, kmid the integer nearest 100 r.
-              const int kmid = min(__float_as_int(lo_hi(fT[k >> 1], k) + 12582912.f) - 0x4B400000, kTabLen - 1);
-              const double gx64 = __dmul_rn((double)(xb + k * xs - P.n2x), h);
-              const double ddx = __dsub_rn(a64.x, gx64);
-              const double r2d = __dadd_rn(__dmul_rn(ddx, ddx), dydz);
-              const int b = (kmid == 0) ? 0 : ((r2d >= P.thr[kmid]) ? kmid : kmid - 1);
-              bits[k] = 0x4B000000u + (uint32_t)b;
-            }
-          }
-        }
-      }
-      const uint32_t tabB = smem_u32(S.tab) - 0x2C000000u;  // address(tab) - 4 * bits(2^23)
-#pragma unroll
-      for (int k = 0; k < kNX / 2; k++) {
-        float2 term = __fmul2_rn(aw, make_float2(fminf(rsv[k].x, cap), fminf(rsv[k].y, cap)));
-        if (DDD) {
-          float2 t;
-          asm("ld.shared.f32 %0, [%1];" : "=f"(t.x) : "r"(tabB + (bits[2 * k] << 2)));
-          asm("ld.shared.f32 %0, [%1];" : "=f"(t.y) : "r"(tabB + (bits[2 * k + 1] << 2)));
-          term = __fmul2_rn(term, t);
-        }
-        if (MODE == kEmapKahan)
-          kahan2(sum[k], cmp[k], term);
-        else
-          sum[k] = __fadd2_rn(sum[k], term);
-      }
+      if (!B.clampMid && !((S.nearMask[j] >> (8 + warp)) & 1u))  // uniform
+        near_exact<DDD, MODE, false>(S, P, slot, j, dyz2, ax, aw, gxn, iy, iz, xb, xs, sum, cmp);
+      else
+        near_exact<DDD, MODE, true>(S, P, slot, j, dyz2, ax, aw, gxn, iy, iz, xb, xs, sum, cmp);
     }
     __syncthreads();  // ring slot and atom lists are free again
   }
