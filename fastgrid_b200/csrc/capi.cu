@@ -903,9 +903,13 @@ int runAffinityChunked(ag_ctx* c, float* host, int nchunks) {
     CK(cudaStreamWaitEvent(c->copyStream, c->evChunk[k], 0));
     const int64_t z0 = 8LL * s0, z1 = std::min<int64_t>(8LL * s1, g.nz);
     const size_t off = (size_t)(z0 * plane), cnt = (size_t)((z1 - z0) * plane);
-    for (int m = 0; m < nm; m++)
-      CK(cudaMemcpyAsync(host + (size_t)m * np + off, dMaps + (size_t)m * np + off, sizeof(float) * cnt,
-                         cudaMemcpyDeviceToHost, c->copyStream));
+    if (s0 == 0 && s1 == slabs) {  // one chunk: the affinity maps are one contiguous block
+      if (nm) CK(cudaMemcpyAsync(host, dMaps, sizeof(float) * nm * np, cudaMemcpyDeviceToHost, c->copyStream));
+    } else {
+      for (int m = 0; m < nm; m++)
+        CK(cudaMemcpyAsync(host + (size_t)m * np + off, dMaps + (size_t)m * np + off, sizeof(float) * cnt,
+                           cudaMemcpyDeviceToHost, c->copyStream));
+    }
     CK(cudaMemcpyAsync(host + (size_t)(nm + 1) * np + off, dDmap + off, sizeof(float) * cnt,
                        cudaMemcpyDeviceToHost, c->copyStream));
   }
@@ -1143,9 +1147,9 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
     // Both passes at once (as ag_compute runs them): the e-map on the
     // high-priority stream, its 17 MB copied back as soon as it is done; the
     // affinity pass, which fills the SMs the e-map's last wave leaves free,
-    // in four z-slab chunks whose rows are copied back while later chunks
-    // run, so that little of the 184 MB of affinity maps is copied after the
-    // last kernel.
+    // in z-slab chunks whose rows are copied back while later chunks
+    // run, so that little of the 184 MB of affinity maps (large configuration)
+    // is copied after the last kernel.
     CK(c->ensureEmapStream());
     CK(cudaEventRecord(c->evFork, c->stream));
     CK(cudaStreamWaitEvent(c->emapStream, c->evFork, 0));
@@ -1156,7 +1160,10 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
     CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
                        cudaMemcpyDeviceToHost, c->emapStream));
     CK(cudaEventRecord(c->evJoin, c->emapStream));
-    e = runAffinityChunked(c, P->pinned, 4);
+    // One chunk per 32 MB of affinity maps, at most four (small jobs: one
+    // copy, no per-chunk calls).
+    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(4, (int64_t)nm * np * 4 / (32 << 20)));
+    e = runAffinityChunked(c, P->pinned, chunks);
     CK(cudaStreamWaitEvent(c->stream, c->evJoin, 0));
     if (e) return e;
   } else {
