@@ -1376,15 +1376,28 @@ extern "C" int ag_batch_compute(ag_batch* b) {
   if (!b->exec) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->ctx->device);
+    // The e-map units and the affinity units are independent: with concurrent
+    // passes the graph holds them as two branches, the e-map's on the
+    // context's high-priority stream, so the affinity kernel's CTAs take the
+    // SMs the e-map kernel's last units leave free.
+    ag_ctx* bc = b->ctx;
+    const bool conc = bc->concurrentPasses != 0;
+    if (conc) CK(bc->ensureEmapStream());
+    cudaStream_t est = conc ? bc->emapStream : st;
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int err = AG_OK;
     // NaN in every checksum slot until the job's e-map writes it.
     if (cudaMemsetAsync(b->checks.p, 0xFF, sizeof(double) * b->sub.size(), st) != cudaSuccess)
       err = fail(AG_E_CUDA, "batch checksum reset failed");
+    if (!err && conc &&
+        (cudaEventRecord(bc->evFork, st) != cudaSuccess || cudaStreamWaitEvent(est, bc->evFork, 0) != cudaSuccess))
+      err = fail(AG_E_CUDA, "batch graph fork failed");
+    if (!err && agk::emap_batch_launch(b->ejobs.p, b->eunits.p, b->ne, b->counters.p, 2 * sms, est) != cudaSuccess)
+      err = fail(AG_E_CUDA, "batch e-map launch failed");
+    if (!err && conc && cudaEventRecord(bc->evJoin, est) != cudaSuccess)
+      err = fail(AG_E_CUDA, "batch graph join failed");
     for (ag_ctx* c : b->sub)
       if (!err) err = prepAffinity(c, st);
-    if (!err && agk::emap_batch_launch(b->ejobs.p, b->eunits.p, b->ne, b->counters.p, 2 * sms, st) != cudaSuccess)
-      err = fail(AG_E_CUDA, "batch e-map launch failed");
     if (!err) {
       const cudaError_t ae =
           b->twoPoint ? agk::aff2_batch_launch(b->a2jobs.p, b->aunits.p, b->na, b->counters.p + 1, b->nmPadMax,
@@ -1393,6 +1406,8 @@ extern "C" int ag_batch_compute(ag_batch* b) {
                                               b->nmapsMax, 2 * sms, st);
       if (ae != cudaSuccess) err = fail(AG_E_CUDA, "batch affinity launch failed");
     }
+    if (conc && cudaStreamWaitEvent(st, bc->evJoin, 0) != cudaSuccess && !err)
+      err = fail(AG_E_CUDA, "batch graph join failed");
     cudaGraph_t g = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (err) {
