@@ -265,3 +265,14 @@ def test_packed_table_tail_reconstructs_the_fp32_table():
         got = (np.float64(aws) * kf + np.float64(awg)).astype(np.float32).astype(np.float64)
         want = float(lw) * t[bins].astype(np.float64) * 2.0 ** -16
         assert np.abs(got / want - 1.0).max() <= 2.0 ** -23
+
+
+def test_python_constants_match_the_header():
+    """Every tuning knob and work flag the header defines is bound in Python
+    with the same value (a knob added to one side only would pass silently)."""
+    txt = open(HEADER).read()
+    defs = dict(re.findall(r"#define\s+(AG_(?:TUNE|WORK|EMAP)_[A-Z0-9_]+)\s+(-?\d+)", txt))
+    assert any(k.startswith("AG_TUNE_") for k in defs)
+    for name, value in defs.items():
+        assert hasattr(fg, name), name
+        assert getattr(fg, name) == int(value), name
