@@ -4,9 +4,10 @@ large synthetic configuration — 20,000 receptor atoms in a 45 x 35 x 30 A
 ellipsoid, 161^3 grid at 0.375 A, ligand types A C HD N NA OA SA S F Cl — on
 the B200 engine.
 
-A step is one map set.  `value` is point-atom evaluations per second over all
-ranks (N_atoms x N_points per map set / map-set seconds), with the inputs
-resident in HBM; `e2e` is the same metric through the public C ABI with host
+A step is one map set (the e-map and the affinity pass run concurrently, as
+the library runs them; each pass is also timed alone for the rooflines).
+`value` is point-atom evaluations per second over all ranks (N_atoms x
+N_points per map set / map-set seconds), with the inputs resident in HBM; `e2e` is the same metric through the public C ABI with host
 buffers (ag_problem_compute: upload, compute, all maps back in host memory).  L2 is flushed (256 MiB
 write) between timed steps.
 
