@@ -1129,9 +1129,21 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
   ag_affinity_params a;
   const double* eps = nullptr;
   ag_problem_views(P, &g, &r, &a, &eps);
-  if (int e = ag_upload(c, &g, &r, &a, eps)) return e;
-  const int64_t np = c->npoints();
   const int nm = p.numMaps();
+  bool anyCovalent = false;
+  for (int m = 0; m < nm; m++) anyCovalent |= p.maps[m].isCovalent;
+  const bool conc = c->concurrentPasses && !anyCovalent;
+  // Sequential order: everything staged first.  Concurrent order: the e-map
+  // is launched as soon as its own inputs are on the device, and the
+  // affinity pass's inputs are staged on the host while it runs.
+  if (conc) {
+    c->haveJob = false;
+    c->haveAff = false;
+    if (int e = stageEmap(c, &g, r.n_atoms, r.xyzw, eps, false)) return e;
+  } else if (int e = ag_upload(c, &g, &r, &a, eps)) {
+    return e;
+  }
+  const int64_t np = c->npoints();
   const size_t total = (size_t)(nm + 2) * np;
   if (P->pinnedN < total) {
     if (P->pinned) cudaFreeHost(P->pinned);
@@ -1140,32 +1152,54 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
     CK(cudaHostAlloc((void**)&P->pinned, sizeof(float) * total, cudaHostAllocDefault));
     P->pinnedN = total;
   }
-  bool anyCovalent = false;
-  for (int m = 0; m < nm; m++) anyCovalent |= p.maps[m].isCovalent;
   CK(c->ensureCopyStream());
-  if (c->concurrentPasses && c->haveAff && useTwoPoint(c) && !anyCovalent) {
+  if (conc) {
     // Both passes at once (as ag_compute runs them): the e-map on the
     // high-priority stream, its 17 MB copied back as soon as it is done; the
     // affinity pass, which fills the SMs the e-map's last wave leaves free,
-    // in z-slab chunks whose rows are copied back while later chunks
-    // run, so that little of the 184 MB of affinity maps (large configuration)
-    // is copied after the last kernel.
+    // in z-slab chunks whose rows are copied back while later chunks run, so
+    // that little of the 184 MB of affinity maps (large configuration) is
+    // copied after the last kernel.
+    c->nMaps = nm;
+    CK(c->maps.ensure(total));
+    CK(cudaMemsetAsync(c->status.p, 0, sizeof(unsigned), c->stream));
     CK(c->ensureEmapStream());
     CK(cudaEventRecord(c->evFork, c->stream));
     CK(cudaStreamWaitEvent(c->emapStream, c->evFork, 0));
     std::swap(c->stream, c->emapStream);
-    int e = ag_compute(c, AG_WORK_EMAP);
+    int e = runEmap(c, c->maps.p + (size_t)nm * np);
     std::swap(c->stream, c->emapStream);
     if (e) return e;
     CK(cudaMemcpyAsync(P->pinned + (size_t)nm * np, c->maps.p + (size_t)nm * np, sizeof(float) * np,
                        cudaMemcpyDeviceToHost, c->emapStream));
     CK(cudaEventRecord(c->evJoin, c->emapStream));
-    // One chunk per 32 MB of affinity maps, at most four (small jobs: one
-    // copy, no per-chunk calls).
-    const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(4, (int64_t)nm * np * 4 / (32 << 20)));
-    e = runAffinityChunked(c, P->pinned, chunks);
+    e = stageAffinity(c, &r, &a);
+    if (!e) {
+      c->haveJob = true;
+      if (useTwoPoint(c)) {
+        // One chunk per 32 MB of affinity maps, at most four (small jobs:
+        // one copy, no per-chunk calls).
+        const int chunks = (int)std::max<int64_t>(1, std::min<int64_t>(4, (int64_t)nm * np * 4 / (32 << 20)));
+        e = runAffinityChunked(c, P->pinned, chunks);
+      } else {
+        e = runAffinity(c, c->maps.p, c->maps.p + (size_t)(nm + 1) * np);
+        if (!e) {
+          CK(cudaEventRecord(c->evAff, c->stream));
+          CK(cudaStreamWaitEvent(c->copyStream, c->evAff, 0));
+          if (nm) CK(cudaMemcpyAsync(P->pinned, c->maps.p, sizeof(float) * nm * np, cudaMemcpyDeviceToHost,
+                                     c->copyStream));
+          CK(cudaMemcpyAsync(P->pinned + (size_t)(nm + 1) * np, c->maps.p + (size_t)(nm + 1) * np,
+                             sizeof(float) * np, cudaMemcpyDeviceToHost, c->copyStream));
+        }
+      }
+    }
+    // Joined on every path: no e-map work may outlive the call.
     CK(cudaStreamWaitEvent(c->stream, c->evJoin, 0));
-    if (e) return e;
+    if (e) {
+      cudaStreamSynchronize(c->stream);
+      cudaStreamSynchronize(c->copyStream);
+      return e;
+    }
   } else {
     // Affinity, d-map and covalent maps first; their copy to the host then
     // runs on a second stream while the e-map (most of the time) is computed.
