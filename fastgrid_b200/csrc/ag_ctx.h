@@ -74,8 +74,9 @@ struct ag_ctx {
   int itemsCompact = -1;      // the order hItems was built with
   bool itemsOnDevice = false; // items / blocks hold hItems / hBlocks
   std::vector<double> epsHost;  // the staged 332/eps table (FP64), empty for the constant dielectric
-  std::vector<double> atomsHost;  // host copy of the staged atoms (x, y, z, w)
+  std::vector<double> atomsHost;  // host copy of the staged atoms (x, y, z, w), read back on demand
   uint64_t atomsVersion = 0;      // bumped whenever new atoms are staged
+  uint64_t atomsHostVersion = ~0ull;  // the staging atomsHost holds
   // affinity
   agc::DevBuf<int> info, cellStart, cellAtoms, cellOf, count, fill, dStart, dAtoms, donorMask, closestH;
   agc::DevBuf<int> ctStart, ctAtoms;  // type-major cell list ((cell, type) segments) of the two-point kernel

@@ -422,8 +422,7 @@ int stageEmap(ag_ctx* c, const ag_grid* g, int n, const double* xyzw, const doub
     }
     CK(c->atoms.ensure(n));
     if (n) CK(cudaMemcpyAsync(c->atoms.p, xyzw, sizeof(double) * 4 * n, cudaMemcpyHostToDevice, c->stream));
-    c->atomsHost.assign(xyzw, xyzw + 4 * (size_t)n);
-    c->atomsVersion++;
+    c->atomsVersion++;  // the surrogate reads the staged atoms back when it needs a host copy
   }
   c->epsHost.clear();
   if (c->ddd) {
@@ -1046,8 +1045,10 @@ struct ag_problem {
   std::vector<double> solparProbe, volProbe;
   float* pinned = nullptr;  // page-locked host copy of the map set (the D2H copies land here)
   size_t pinnedN = 0;
+  const void* xyzwLocked = nullptr;  // p.xyzw, page-locked once for fast uploads (it never moves after loading)
   ~ag_problem() {
     if (pinned) cudaFreeHost(pinned);
+    if (xyzwLocked) cudaHostUnregister(const_cast<void*>(xyzwLocked));
   }
 };
 
@@ -1129,6 +1130,12 @@ extern "C" int ag_problem_compute(ag_ctx* c, ag_problem* P) {
   ag_affinity_params a;
   const double* eps = nullptr;
   ag_problem_views(P, &g, &r, &a, &eps);
+  // The atoms are this call's largest upload: page-lock them once so that
+  // each call copies them by DMA (a failure only leaves the copy slower).
+  if (!P->xyzwLocked && !p.xyzw.empty() &&
+      cudaHostRegister(p.xyzw.data(), sizeof(double) * p.xyzw.size(), cudaHostRegisterPortable) == cudaSuccess)
+    P->xyzwLocked = p.xyzw.data();
+  cudaGetLastError();  // clear a failed registration
   const int nm = p.numMaps();
   bool anyCovalent = false;
   for (int m = 0; m < nm; m++) anyCovalent |= p.maps[m].isCovalent;

@@ -251,7 +251,13 @@ int surrPrepare(ag_ctx* c, SurrState& S) {
   }
   if (S.sortedVersion != c->atomsVersion) {
     const int n = c->nAtoms;
-    if ((int64_t)c->atomsHost.size() != 4 * (int64_t)n) return fail(AG_E_INVALID, "staged atoms have no host copy");
+    if (c->atomsHostVersion != c->atomsVersion) {  // host copy of the staged atoms, read back once per staging
+      c->atomsHost.resize(4 * (size_t)n);
+      if (n) CK(cudaMemcpyAsync(c->atomsHost.data(), c->atoms.p, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost,
+                                c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      c->atomsHostVersion = c->atomsVersion;
+    }
     const double* x = c->atomsHost.data();
     std::vector<std::pair<uint32_t, int>> order(n);
     for (int i = 0; i < n; i++) {
