@@ -18,7 +18,10 @@
 //    atom's distance d to the CTA's box into three lists:
 //      near (d < rNear): 1/r capped at 2, Kahan-compensated per pair, and the
 //        bin decided exactly in FP64 (squared-distance threshold table) when
-//        100 r lies within `delta` of a bin edge;
+//        100 r lies within `delta` of a bin edge.  Decided again per warp:
+//        a warp whose own points are all at least rNear away evaluates the
+//        atom with the mid arithmetic (each term still compensated), and the
+//        cap and the table clamp are dropped where they cannot apply;
 //      mid (rNear <= d < rFar): bin by a round-down FMA, table read;
 //      far (d >= rFar, at least 50 A): the table has saturated there (its
 //        entries differ from entry 8191 by < 2e-6 relative), so the term is
