@@ -180,7 +180,10 @@ int ag_problem_info_get(const ag_problem* p, ag_problem_info* info);
 /* Views of the host arrays the GPU consumes (valid while p lives). */
 int ag_problem_views(const ag_problem* p, ag_grid* grid, ag_receptor* rec, ag_affinity_params* par,
                      const double** inv_eps);
-/* Compute the whole map set on the GPU (also covalent maps and the floating grid). */
+/* Compute the whole map set on the GPU (also covalent maps and the floating grid).
+ * Synchronous: the maps are in host memory (ag_problem_maps) when it returns.
+ * The problem keeps a page-locked buffer for the maps, and its atom array is
+ * page-locked on the first call; both are released by ag_problem_free. */
 int ag_problem_compute(ag_ctx* ctx, ag_problem* p);
 /* Host copy of the map set [n_maps][e][d], FP32 unrounded; n*(n_maps+2) floats. */
 const float* ag_problem_maps(const ag_problem* p);
