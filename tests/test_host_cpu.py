@@ -276,3 +276,20 @@ def test_python_constants_match_the_header():
     for name, value in defs.items():
         assert hasattr(fg, name), name
         assert getattr(fg, name) == int(value), name
+
+
+def test_bench_affinity_pair_count_is_exact():
+    """bench.py's count of (grid point, atom) pairs within 8 A (the affinity
+    pass's algorithmic work in the map set's FP32 roofline) equals a brute
+    force count, atoms inside, on and outside the grid."""
+    sys.path.insert(0, REPO)
+    import bench
+
+    rng = np.random.default_rng(12)
+    nx, ny, nz, h = 23, 17, 20, 0.5
+    xyz = np.concatenate([rng.uniform(-9, 9, (150, 3)), rng.uniform(-16, 16, (60, 3))])
+    xyz[:5] = (np.array([[0, 0, 0], [2, -3, 1], [4, 4, 4], [-5, 0, 2], [1, 1, -1]]) * h)  # on grid points
+    g = np.stack(np.meshgrid((np.arange(nx) - nx // 2) * h, (np.arange(ny) - ny // 2) * h,
+                             (np.arange(nz) - nz // 2) * h, indexing="ij"), -1).reshape(-1, 3)
+    brute = sum(int((((g - a) ** 2).sum(1) <= 64.0).sum()) for a in xyz)
+    assert bench.affinity_pairs(xyz, nx, ny, nz, h) == brute
